@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark of the matrix-free p = 2 B-spline elasticity PCG on B200.
+
+Workload (default): the SIMP cantilever on 128 x 64 x 64 elements (1,698,840 DOF), box
+[0,2]x[0,1]x[0,1], densities i.i.d. U[0.01,1] smoothed by a 3x3x3 box filter (seeded PCG64),
+E0 = 1, E_min = 1e-9, nu = 0.3, SIMP penalty 3, x = 0 clamped, unit downward traction on x = 2.
+One step = one Jacobi-PCG solve to relative residual 1e-8 from x = 0.
+
+value    = DOF * iterations / device seconds of the solve, inputs resident in HBM (CUDA events on
+           the solver's stream, L2 flushed between steps), summed over ranks (replicas).
+e2e      = the same metric through the host-pointer C ABI call (icc_op_update_scale +
+           icc_pcg_solve): H2D of the step's scale and load, D2H of the solution, inside the timing.
+roofline = the FP64 brick contraction kernel: algorithmic 2*81*81 flops per element per launch
+           over its mean CUDA-event duration, against this run's measured FP64 DMMA peak
+           (cuBLAS DGEMM through torch.matmul on float64, 8192^3).
+cpu_baseline / --impl reference = the oracle (C restatement of the reference's CPU path:
+           element-loop operator with OpenMP, serial PCG vector loops) on the host cores, a
+           bounded number of PCG iterations of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PCG time-to-1e-8 & DOF·iter/s, mixed vs FP64 on 1 B200; err vs FP64 oracle"
+UNIT = "DOF*iter/s"
+TOL = 1e-8
+SEED = 2026
+WORKLOADS = {
+    "cantilever128": dict(nel=(128, 64, 64), smooth=True),
+    "cantilever24": dict(nel=(24, 16, 12), smooth=False),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cantilever128", choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-solution", action="store_true", help="skip the tight FP64 error reference")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_tensor_peak(torch, dev):
+    """Measured FP64 tensor-core peak of this GPU: cuBLAS DGEMM (torch.matmul float64), TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_sample(problem, seconds, oracle_mod):
+    """Oracle (reference CPU path restated in C) PCG iterations on the host for ~seconds."""
+    O = oracle_mod
+    osp = O.Space(problem.bounds, problem.nel, 2)
+    lam, mu = O.lame(1.0, 0.3)
+    types, tid, _ = osp.element_matrices(lam, mu)
+    b = np.where(problem.free_mask > 0, problem.force, 0.0)
+    diag = np.maximum(O.mf_diagonal(osp, types, tid, problem.scale), 1e-12)
+    t0 = time.perf_counter()
+    O.pcg_mf(osp, types, tid, problem.scale, b, diag, 1, 0.0, problem.free_mask, 1)
+    t_one = time.perf_counter() - t0
+    iters = int(max(2, min(500, seconds / max(t_one, 1e-6))))
+    t0 = time.perf_counter()
+    x, it, res = O.pcg_mf(osp, types, tid, problem.scale, b, diag, iters, 0.0, problem.free_mask, 1)
+    dt = time.perf_counter() - t0
+    return {"value": problem.ndof * it / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{it} Jacobi-PCG iterations of {problem.name} ({problem.ndof} DOF) with the oracle's "
+                      f"matrix-free element-loop operator (OpenMP) and serial vector loops, {dt:.1f} s",
+            "seconds": dt}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from immersed_catmull_clark_b200 import workloads as W
+    from oracle import oracle as O
+    O.build()
+    wl = WORKLOADS[args.workload]
+    prob = W.cantilever(wl["nel"], smooth=wl["smooth"], seed=SEED)
+    per_step = max(2.0, min(60.0, args.cpu_seconds))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_sample(prob, per_step, O)
+        if i >= args.warmup:
+            vals.append(s)
+    value = float(np.mean([s["value"] for s in vals]))
+    ms = float(np.mean([s["seconds"] for s in vals]) * 1e3)
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+           "config": {"workload": prob.name, "ndof": prob.ndof, "tol": TOL, "seed": SEED},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[0]["cores"], "kind": "port",
+                            "sample": vals[0]["sample"]},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    import immersed_catmull_clark_b200 as icc
+    from immersed_catmull_clark_b200 import workloads as W
+
+    wl = WORKLOADS[args.workload]
+    prob = W.cantilever(wl["nel"], smooth=wl["smooth"], seed=SEED + rank)
+    sp = icc.SpaceBox(prob.bounds, prob.nel, 2)
+    lam, mu = icc.lame(W.E0, W.NU)
+    em = icc.elasticity_element_matrices(sp, lam, mu)
+    op = icc.MatrixFreeOperator(sp, em, prob.scale, prob.free_mask, icc.MASK_ZERO)
+    n = sp.ndof
+    stream = torch.cuda.ExternalStream(op.stream, device=dev)
+    b_host = W.rhs_masked(prob)
+    b_dev = torch.from_numpy(b_host).to(dev)
+    x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+    precision = icc.MIXED if args.mode == "mixed" else icc.FP64
+    solver = icc.PcgSolver(20 * n, TOL, precision=precision)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        solver.solve_dev(n, b_dev.data_ptr(), 0, x_dev.data_ptr(), op)
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    iters, launches = [], 0
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev[i][0].record(stream)
+            it, res = solver.solve_dev(n, b_dev.data_ptr(), 0, x_dev.data_ptr(), op)
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+            iters.append(it)
+            launches += op.last_solve_info().kernel_launches
+        barrier()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    t_ms = float(np.sum(ms_steps))
+    local_value = n * float(np.sum(iters)) / (t_ms * 1e-3)
+    info = op.last_solve_info()
+
+    # roofline of the dominant kernel (FP64 brick contraction), timed on the solver's stream
+    y_dev = torch.empty_like(x_dev)
+    p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev)
+    contract_ms, gather_ms = op.profile_apply(p_dev.data_ptr(), y_dev.data_ptr(), 20)
+    flops = 2.0 * 81 * 81 * sp.nel
+    achieved = flops / (contract_ms * 1e-3) / 1e12
+    peak = fp64_tensor_peak(torch, dev)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            t = json.load(open(tpath)).get("apply_f64_kernel", {}).get(args.workload)
+            traffic = None if t is None else float(t)
+        except Exception:
+            traffic = None
+
+    # end to end through the host-pointer C ABI (pinned host buffers)
+    b_pin = torch.from_numpy(b_host).pin_memory()
+    s_pin = torch.from_numpy(prob.scale.copy()).pin_memory()
+    x_pin = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    e2e_ms, e2e_it = 0.0, 0
+    for _ in range(e2e_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0.record(stream)
+        op.update_scale(s_pin.numpy())
+        it, res = solver.solve_host_ptr(n, b_pin.numpy(), None, x_pin.numpy(), op)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        e2e_it += it
+    e2e_local = n * e2e_it / (e2e_ms * 1e-3)
+
+    # accuracy against a tight FP64 solution (FP64 device PCG at 1e-12)
+    err = {}
+    if not args.no_ref_solution:
+        x_ref = torch.zeros_like(x_dev)
+        ref_solver = icc.PcgSolver(40 * n, 1e-12, precision=icc.FP64)
+        it_ref, res_ref = ref_solver.solve_dev(n, b_dev.data_ptr(), 0, x_ref.data_ptr(), op)
+        xr, xs = x_ref.cpu().numpy(), x_dev.cpu().numpy()
+        c_ref, c = float(prob.force @ xr), float(prob.force @ xs)
+        err = {"disp_rel_l2": float(np.linalg.norm(xs - xr) / np.linalg.norm(xr)),
+               "compliance_rel": abs(c - c_ref) / abs(c_ref), "ref": f"FP64 device PCG to {res_ref:.1e} ({it_ref} it)"}
+
+    # max over ranks of time, sum of throughput
+    if world > 1:
+        tt = torch.tensor([t_ms, local_value, e2e_local], dtype=torch.float64, device=dev)
+        mx = tt.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = tt.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        t_ms_all = float(mx[0]); value = n * float(np.sum(iters)) * world / (t_ms_all * 1e-3)
+        e2e_value = float(sm[2])
+    else:
+        t_ms_all, value, e2e_value = t_ms, local_value, e2e_local
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import oracle as O
+        O.build()
+        cpu = cpu_sample(prob, args.cpu_seconds, O)
+        cpu.pop("seconds", None)
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": t_ms_all / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == icc.FP64 else "tf32x3+f32+f64",
+               "data": "synthetic",
+               "config": {"workload": f"{prob.name} SIMP cantilever, smoothed densities" if wl["smooth"] else prob.name,
+                          "ndof": n, "nel": sp.nel, "tol": TOL, "seed": SEED, "mode": args.mode,
+                          "iterations": iters, "time_to_tol_ms": ms_steps,
+                          "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+               "roofline": {"bound": "tensor", "kernel": "apply_f64_kernel (FP64 DMMA)", "achieved": achieved,
+                            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                            "algorithmic_flops_per_launch": flops, "launch_ms": contract_ms,
+                            "node_sum_kernel_ms": gather_ms,
+                            "peak_source": "measured in this run: cuBLAS DGEMM (torch.matmul float64 8192^3), "
+                                           "FP64 is absent from MEASURED_PEAKS.json"},
+               "cpu_baseline": cpu,
+               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n + 8 * sp.nel,
+                       "d2h_bytes_per_step": 8 * n},
+               "gpu_launches": int(launches),
+               "clocks": clk.summary(),
+               "accuracy": err,
+               "solve_info": {"rel_res": info.rel_res, "device_ms": info.device_ms}}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

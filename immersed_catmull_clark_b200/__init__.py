@@ -1,0 +1,276 @@
+"""B200 matrix-free p = 2 B-spline elasticity operator and Jacobi-PCG, behind a C ABI.
+
+Python front end (ctypes) of libicc.so, shaped like the reference's Rust API so callers and
+tests read the same:
+
+* ``SpaceBox(bounds, nsub, 2)``                      rust/src/iga/space.rs:107 SpaceBox::new
+* ``lame(young, poisson)``                           rust/src/iga/elasticity.rs:173
+* ``elasticity_element_matrices(sp, lam, mu)``       rust/src/iga/elasticity.rs:30
+* ``MatrixFreeOperator(sp, em, scale, ...)``         replaces AssemblyPattern::assemble +
+  CsrMatrix::{matvec, diagonal} (rust/src/sparse.rs:160, :60, :70) with the device operator
+* ``PcgSolver(max_iter, tol).solve(n, b, diag, op)`` rust/src/solver.rs:9-76; the closure
+  argument is the operator handle (its mask mode selects the reference's closure)
+
+All compute runs in libicc's CUDA kernels.  There is no CPU fallback: without the built
+library or a B200 the calls raise ``IccError``.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libicc.so")
+
+ICC_OK = 0
+ICC_NOT_CONVERGED = 1
+ICC_BREAKDOWN = 2
+ICC_BAD_ARG = -1
+ICC_CUDA_ERROR = -2
+ICC_TIMEOUT = -3
+ICC_NO_DEVICE = -4
+ICC_OUT_OF_MEMORY = -5
+ICC_NAN = -6
+
+MASK_NONE, MASK_ZERO, MASK_IDENTITY = 0, 1, 2
+FP64, MIXED = 0, 1
+
+# every symbol include/icc.h declares
+EXPORTED = [
+    "icc_last_error", "icc_space_create", "icc_space_destroy", "icc_space_dims", "icc_space_connectivity",
+    "icc_lame", "icc_element_matrices", "icc_op_create", "icc_op_create_lame", "icc_op_destroy",
+    "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_diagonal",
+    "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
+]
+
+
+class IccError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"icc error {code}: {msg}")
+        self.code = code
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("check_every", C.c_int32), ("inner_tol", C.c_double),
+                ("max_outer", C.c_int32), ("reserved", C.c_int32)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("outer_iterations", C.c_int64), ("rel_res", C.c_double),
+                ("device_ms", C.c_double), ("fp64_applies", C.c_int64), ("mixed_applies", C.c_int64),
+                ("kernel_launches", C.c_int64)]
+
+
+_lib = None
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def lib():
+    """Load libicc.so (built in-tree by __graft_entry__.build or immersed_catmull_clark_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise IccError(ICC_NO_DEVICE, f"{LIB_PATH} is not built (run immersed_catmull_clark_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    L.icc_last_error.restype = C.c_char_p
+    L.icc_space_create.argtypes = [f64p, i64p, i32, C.POINTER(vp)]
+    L.icc_space_destroy.argtypes = [vp]
+    L.icc_space_dims.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), i64p, i64p]
+    L.icc_space_connectivity.argtypes = [vp, i64p]
+    L.icc_lame.argtypes = [dbl, dbl, C.POINTER(dbl), C.POINTER(dbl)]
+    L.icc_lame.restype = None
+    L.icc_element_matrices.argtypes = [vp, dbl, dbl, vp, i32, vp, C.POINTER(i32)]
+    L.icc_op_create.argtypes = [vp, f64p, i32, i32p, vp, vp, i32, C.POINTER(vp)]
+    L.icc_op_create_lame.argtypes = [vp, dbl, dbl, vp, vp, i32, C.POINTER(vp)]
+    L.icc_op_destroy.argtypes = [vp]
+    L.icc_op_destroy.restype = None
+    L.icc_op_update_scale.argtypes = [vp, vp]
+    L.icc_op_update_mask.argtypes = [vp, vp, i32]
+    L.icc_op_apply.argtypes = [vp, f64p, f64p, i64]
+    L.icc_op_apply_dev.argtypes = [vp, vp, vp, i64]
+    L.icc_op_diagonal.argtypes = [vp, f64p, i64]
+    L.icc_op_stream.argtypes = [vp]
+    L.icc_op_stream.restype = vp
+    L.icc_pcg_solve.argtypes = [vp, f64p, vp, i64, dbl, i64, C.POINTER(SolveOpts), f64p,
+                                C.POINTER(i64), C.POINTER(dbl)]
+    L.icc_pcg_solve_dev.argtypes = [vp, vp, vp, i64, dbl, i64, C.POINTER(SolveOpts), vp,
+                                    C.POINTER(i64), C.POINTER(dbl)]
+    L.icc_op_last_solve_info.argtypes = [vp, C.POINTER(SolveInfo)]
+    L.icc_op_profile_apply.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
+    _lib = L
+    return L
+
+
+def _check(rc, allow=(ICC_OK,)):
+    if rc in allow:
+        return rc
+    raise IccError(rc, lib().icc_last_error().decode())
+
+
+def _vp(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def lame(young, poisson):
+    lam, mu = C.c_double(), C.c_double()
+    lib().icc_lame(young, poisson, C.byref(lam), C.byref(mu))
+    return lam.value, mu.value
+
+
+class SpaceBox:
+    """p = 2 tensor-product B-spline space on a 3-D box (rust/src/iga/space.rs:107)."""
+
+    def __init__(self, bounds, nsub, degree=2):
+        b = np.ascontiguousarray(np.asarray(bounds, dtype=np.float64).reshape(-1))
+        ns = np.ascontiguousarray(np.asarray(nsub, dtype=np.int64))
+        h = C.c_void_p()
+        _check(lib().icc_space_create(b, ns, int(degree), C.byref(h)))
+        self._h = h
+        ndof, nel = C.c_int64(), C.c_int64()
+        nd = np.zeros(3, dtype=np.int64); ne = np.zeros(3, dtype=np.int64)
+        _check(lib().icc_space_dims(h, C.byref(ndof), C.byref(nel), nd, ne))
+        self.ndof, self.nel = ndof.value, nel.value
+        self.ndof_dir = [int(v) for v in nd]
+        self.nel_dir = [int(v) for v in ne]
+        self.ndof_sc = self.ndof // 3
+        self.nsh = 81
+        self.bounds = np.asarray(bounds, dtype=np.float64).reshape(3, 2)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.icc_space_destroy(h)
+            self._h = None
+
+    def connectivity(self):
+        c = np.zeros(self.nel * 81, dtype=np.int64)
+        _check(lib().icc_space_connectivity(self._h, c))
+        return c
+
+
+@dataclass
+class ElementMatrices:
+    """rust/src/iga/elasticity.rs:14-26: distinct 81x81 matrices and the type of every element."""
+    types: np.ndarray     # [ntypes, 81, 81] float64
+    type_id: np.ndarray   # [nel] int32
+
+
+def elasticity_element_matrices(sp, lam, mu):
+    nt = C.c_int32()
+    _check(lib().icc_element_matrices(sp._h, lam, mu, None, 0, None, C.byref(nt)))
+    types = np.zeros((nt.value, 81, 81))
+    tid = np.zeros(sp.nel, dtype=np.int32)
+    _check(lib().icc_element_matrices(sp._h, lam, mu, _vp(types), nt.value, _vp(tid), C.byref(nt)))
+    return ElementMatrices(types, tid)
+
+
+class MatrixFreeOperator:
+    """Device operator y = A x, A = the masked sum_e s_e K_type(e) (replaces the assembled CSR)."""
+
+    def __init__(self, sp, em, scale=None, free_mask=None, mask_mode=MASK_NONE):
+        self.sp = sp
+        self.n = sp.ndof
+        h = C.c_void_p()
+        s = None if scale is None else np.ascontiguousarray(scale, dtype=np.float64)
+        fm = None if free_mask is None else np.ascontiguousarray(free_mask, dtype=np.uint8)
+        if isinstance(em, ElementMatrices):
+            types = np.ascontiguousarray(em.types, dtype=np.float64).reshape(-1)
+            tid = np.ascontiguousarray(em.type_id, dtype=np.int32)
+            rc = lib().icc_op_create(sp._h, types, len(em.types), tid, _vp(s), _vp(fm), mask_mode, C.byref(h))
+        else:
+            lam, mu = em
+            rc = lib().icc_op_create_lame(sp._h, lam, mu, _vp(s), _vp(fm), mask_mode, C.byref(h))
+        _check(rc)
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.icc_op_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def stream(self):
+        return lib().icc_op_stream(self._h)
+
+    def update_scale(self, scale):
+        s = None if scale is None else np.ascontiguousarray(scale, dtype=np.float64)
+        _check(lib().icc_op_update_scale(self._h, _vp(s)))
+
+    def update_mask(self, free_mask, mask_mode):
+        fm = None if free_mask is None else np.ascontiguousarray(free_mask, dtype=np.uint8)
+        _check(lib().icc_op_update_mask(self._h, _vp(fm), mask_mode))
+
+    def matvec(self, x):
+        y = np.zeros(self.n)
+        _check(lib().icc_op_apply(self._h, np.ascontiguousarray(x, dtype=np.float64), y, self.n))
+        return y
+
+    def matvec_dev(self, x_ptr, y_ptr):
+        """Device pointers (e.g. torch tensor .data_ptr()); enqueued on the operator's stream."""
+        _check(lib().icc_op_apply_dev(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), self.n))
+
+    def diagonal(self):
+        d = np.zeros(self.n)
+        _check(lib().icc_op_diagonal(self._h, d, self.n))
+        return d
+
+    def profile_apply(self, x_ptr, y_ptr, reps=20):
+        """Mean device ms of (brick contraction kernel, node-sum kernel) over reps FP64 applies."""
+        a, g = C.c_double(), C.c_double()
+        _check(lib().icc_op_profile_apply(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), reps, C.byref(a),
+                                          C.byref(g)))
+        return a.value, g.value
+
+    def last_solve_info(self):
+        info = SolveInfo()
+        _check(lib().icc_op_last_solve_info(self._h, C.byref(info)))
+        return info
+
+
+class PcgSolver:
+    """rust/src/solver.rs:9-76 PcgSolver on the device operator.
+
+    precision FP64 reproduces the reference loop in FP64; MIXED runs FP64 iterative refinement
+    around a tensor-core FP32 inner PCG.  ``solve`` returns (x, iters, rel_res) like the
+    reference; ``status`` holds the C status (ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN).
+    """
+
+    def __init__(self, max_iter, tol, precision=FP64, check_every=32, inner_tol=0.0, max_outer=0):
+        self.max_iter, self.tol = int(max_iter), float(tol)
+        self.opts = SolveOpts(precision, check_every, inner_tol, max_outer, 0)
+        self.status = None
+
+    def solve(self, n, b, diag_a, op):
+        x = np.zeros(n)
+        it, res = C.c_int64(), C.c_double()
+        d = None if diag_a is None else np.ascontiguousarray(diag_a, dtype=np.float64)
+        rc = lib().icc_pcg_solve(op._h, np.ascontiguousarray(b, dtype=np.float64), _vp(d), n, self.tol,
+                                 self.max_iter, C.byref(self.opts), x, C.byref(it), C.byref(res))
+        self.status = _check(rc, (ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN))
+        return x, it.value, res.value
+
+    def solve_host_ptr(self, n, b, diag_a, x, op):
+        """Like solve() but writes into the caller's host array x (e.g. pinned memory)."""
+        it, res = C.c_int64(), C.c_double()
+        d = None if diag_a is None else np.ascontiguousarray(diag_a, dtype=np.float64)
+        rc = lib().icc_pcg_solve(op._h, b, _vp(d), n, self.tol, self.max_iter, C.byref(self.opts), x,
+                                 C.byref(it), C.byref(res))
+        self.status = _check(rc, (ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN))
+        return it.value, res.value
+
+    def solve_dev(self, n, b_ptr, diag_ptr, x_ptr, op):
+        it, res = C.c_int64(), C.c_double()
+        rc = lib().icc_pcg_solve_dev(op._h, C.c_void_p(b_ptr), C.c_void_p(diag_ptr) if diag_ptr else None, n,
+                                     self.tol, self.max_iter, C.byref(self.opts), C.c_void_p(x_ptr),
+                                     C.byref(it), C.byref(res))
+        self.status = _check(rc, (ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN))
+        return it.value, res.value

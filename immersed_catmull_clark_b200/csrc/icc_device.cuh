@@ -1,0 +1,131 @@
+// Device-side declarations: brick geometry, solver state, the operator handle and small
+// device helpers shared by the FP64 (icc_op.cu) and tensor-core mixed (icc_mixed.cu) paths.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "icc_internal.h"
+
+namespace icc {
+
+// Brick of elements owned by one CTA and its control-point patch.
+constexpr int kBX = 8, kBY = 4, kBZ = 4;
+constexpr int kPX = kBX + 2, kPY = kBY + 2, kPZ = kBZ + 2;
+constexpr int kPVol = kPX * kPY * kPZ;  // 360 control points per component
+constexpr int kEPB = kBX * kBY * kBZ;   // 128 elements per brick
+
+// FP64 DMMA tiling of the 81x81 contraction: K (trial) padded to 84 = 21 x 4, N (test) to 88 = 11 x 8.
+constexpr int kKSteps = 21;
+constexpr int kNTiles = 11;
+constexpr int kFragPerType = kKSteps * kNTiles * 32;
+constexpr int kApplyThreads = 256;
+constexpr int kApplySmem = (3 * kPVol + kEPB * 81) * 8;
+
+constexpr int kVecThreads = 256;
+
+// PCG stop states (rust/src/solver.rs:40-73)
+constexpr int kStatConverged = 1;
+constexpr int kStatBreakdown = 2;
+constexpr int kStatMaxIter = 3;
+constexpr int kStatNan = 4;
+
+struct Geom {
+    int nx, ny, nz;        // elements per direction
+    int cx, cy, cz;        // control points per direction
+    long long nsc;         // scalar control points
+    int nbx, nby, nbz;     // bricks per direction
+    int nbricks;
+};
+
+struct PcgState {
+    double rz_old, p_ap, alpha, beta, norm_b, rel_res, tol;
+    long long iter, max_iter;
+    int status, pad;
+};
+
+struct MixedState;  // tensor-core path (icc_mixed.cu)
+
+struct Op {
+    int device = 0, num_sms = 148, vec_blocks = 592;
+    Geom g{};
+    int64_t nel = 0, ndof = 0;
+    int ntypes = 0, ntiles = 0, mask_mode = 0;
+    long long scale_version = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // operator data
+    double *d_scale = nullptr, *d_kfrag = nullptr, *d_kdiag = nullptr;
+    int *d_type_id = nullptr, *d_tile_start = nullptr, *d_tile_type = nullptr;
+    uint8_t *d_tile_elem = nullptr, *d_mask = nullptr;
+    double *d_patch = nullptr;              // brick patch partial sums [nbricks][3][kPVol]
+    double *d_x_in = nullptr, *d_y_out = nullptr;
+    // PCG
+    double *d_x = nullptr, *d_r = nullptr, *d_p = nullptr, *d_ap = nullptr, *d_inv = nullptr, *d_b = nullptr,
+           *d_diag = nullptr, *d_partials = nullptr;
+    PcgState *d_state = nullptr, *h_state = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_batch = 0;
+    icc_solve_info last_info{};
+    // host copies used by the tensor-core path set-up
+    std::vector<double> host_ktypes, host_scale;
+    std::vector<int32_t> host_type_id;
+    MixedState *mixed = nullptr;
+
+    ~Op();
+    int init(const Space &s, const double *ke_types, int nt, const int32_t *type_id, const double *scale,
+             const uint8_t *free_mask, int mode);
+    int set_scale(const double *scale);
+    int set_mask(const uint8_t *free_mask, int mode);
+    void enqueue_apply(const double *x, double *y, double *partials, const PcgState *st);
+    int apply_dev(const double *x, double *y);
+    int diagonal_dev(double *d);
+    int ensure_pcg_buffers();
+    void enqueue_pcg_iteration();
+    int pcg_fp64(const double *b, const double *diag, double tol, int64_t max_iter, int check_every, double *x,
+                 int64_t *iters, double *rel_res);
+};
+
+int cuda_fail(cudaError_t e, const char *where);
+
+// tensor-core mixed-precision path (icc_mixed.cu)
+void mixed_release(Op &op);
+int mixed_on_scale_update(Op &op);
+int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter,
+                const icc_solve_opts &opts, double *x, int64_t *iters, double *rel_res);
+
+// ---- device helpers -------------------------------------------------------------------------
+
+// D[16x8] += A[16x4] * B[4x8] on the FP64 tensor cores.  Fragments (PTX ISA, mma.m16n8k4 .f64):
+// a0/a1 = A[gid][tig] / A[gid+8][tig], b0 = B[tig][gid], d0..d3 = D[gid (+8 for d2,d3)][2 tig + (i&1)],
+// with gid = lane / 4 and tig = lane % 4.
+__device__ __forceinline__ void dmma_m16n8k4(double (&d)[4], double a0, double a1, double b0) {
+    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block reduction; the result is valid in warp 0 (thread 0 writes it out).
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double ws[32];
+    v = warp_sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x < 32) {
+        r = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+}  // namespace icc

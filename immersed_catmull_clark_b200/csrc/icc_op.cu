@@ -1,0 +1,806 @@
+// Matrix-free p = 2 B-spline elasticity operator, Jacobi diagonal and device PCG for sm_100a.
+//
+// Work decomposition.  The element grid is cut into bricks of BX x BY x BZ = 8 x 4 x 4
+// elements.  One CTA owns one brick:
+//   1. it stages the brick's (BX+2)(BY+2)(BZ+2) control-point patch of the input vector, all
+//      three components, into shared memory (input mask applied on the fly);
+//   2. its warps contract the gathered element vectors with the element matrices on the FP64
+//      tensor cores (DMMA, mma.sync m16n8k4 f64): a warp tile is 16 elements of one type,
+//      Y^T[16 x 88] = U^T[16 x 84] * K_type^T[84 x 88] (81 padded to 84 / 88);
+//   3. rows are scaled by s_e, staged in shared memory, and every patch node sums its <= 27
+//      element contributions in a fixed order;
+//   4. the brick's patch partial sums go to a scratch buffer; a node-centric pass then adds the
+//      <= 8 partials of the bricks that share each node (2-plane overlaps), applies the output
+//      mask and, inside PCG, also forms p'Ap.  No atomics anywhere: results are bitwise
+//      reproducible run to run.
+// The reference computes the same y = sum_e s_e K_e u_e through an assembled CSR matrix
+// (rust/src/sparse.rs:128-175 then :60-68).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "icc_internal.h"
+#include "icc_device.cuh"
+
+namespace icc {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(ICC_OUT_OF_MEMORY, std::string(where) + ": " + cudaGetErrorString(e));
+    return set_error(ICC_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define ICC_CUDA(call, where)                         \
+    do {                                              \
+        cudaError_t _e = (call);                      \
+        if (_e != cudaSuccess) return ::icc::cuda_fail(_e, where); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// Device kernels
+// ------------------------------------------------------------------------------------------
+
+// FP64 brick apply.  Writes the brick's patch partial sums to patch_out[brick][3][PVOL].
+__global__ void __launch_bounds__(kApplyThreads, 2)
+apply_f64_kernel(Geom g, const double *__restrict__ x, const uint8_t *__restrict__ mask, int mask_in,
+                 const double *__restrict__ scale, const double *__restrict__ kfrag,
+                 const int *__restrict__ tile_start, const int *__restrict__ tile_type,
+                 const uint8_t *__restrict__ tile_elem, double *__restrict__ patch_out,
+                 const PcgState *__restrict__ st) {
+    if (st && st->status != 0) return;
+    extern __shared__ double smem[];
+    double *sx = smem;                  // [3][PVOL]
+    double *sy = smem + 3 * kPVol;      // [kEPB][81]
+    __shared__ int koff[84];
+
+    const int b = blockIdx.x;
+    const int bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / (g.nbx * g.nby);
+    const int x0 = bxi * kBX, y0 = byi * kBY, z0 = bzi * kBZ;
+    const int ex_n = min(kBX, g.nx - x0), ey_n = min(kBY, g.ny - y0), ez_n = min(kBZ, g.nz - z0);
+
+    if (threadIdx.x < 84) {
+        int k = threadIdx.x;
+        int kk = k < 81 ? k : 0;  // padded k has a zero B row; any in-range A value works
+        int c = kk / 27, a = kk % 27;
+        koff[k] = c * kPVol + ((a / 9) * kPY + (a / 3) % 3) * kPX + a % 3;
+    }
+    for (int i = threadIdx.x; i < 3 * kPVol; i += blockDim.x) {
+        int c = i / kPVol, r = i - c * kPVol;
+        int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
+        int gx = x0 + px, gy = y0 + py, gz = z0 + pz;
+        double v = 0.0;
+        if (gx < g.cx && gy < g.cy && gz < g.cz) {
+            long long idx = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + gx;
+            v = x[idx];
+            if (mask_in && !mask[idx]) v = 0.0;
+        }
+        sx[i] = v;
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int t0 = tile_start[b], t1 = tile_start[b + 1];
+    for (int t = t0 + warp; t < t1; t += kApplyThreads / 32) {
+        const double *kf = kfrag + (size_t)tile_type[t] * kFragPerType;
+        const int e0 = tile_elem[t * 16 + gid], e1 = tile_elem[t * 16 + gid + 8];
+        const int base0 = e0 < kEPB ? ((e0 / (kBX * kBY)) * kPY + (e0 / kBX) % kBY) * kPX + e0 % kBX : 0;
+        const int base1 = e1 < kEPB ? ((e1 / (kBX * kBY)) * kPY + (e1 / kBX) % kBY) * kPX + e1 % kBX : 0;
+        double acc[kNTiles][4];
+#pragma unroll
+        for (int nt = 0; nt < kNTiles; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0;
+#pragma unroll 3
+        for (int ks = 0; ks < kKSteps; ++ks) {
+            const int off = koff[ks * 4 + tig];
+            const double a0 = sx[base0 + off];
+            const double a1 = sx[base1 + off];
+            const double *kk = kf + ks * (kNTiles * 32) + lane;
+#pragma unroll
+            for (int nt = 0; nt < kNTiles; ++nt) {
+                const double bf = __ldg(kk + nt * 32);
+                dmma_m16n8k4(acc[nt], a0, a1, bf);
+            }
+        }
+        const int zx0 = (b % g.nbx) * kBX, zy0 = ((b / g.nbx) % g.nby) * kBY, zz0 = (b / (g.nbx * g.nby)) * kBZ;
+        double s0 = 0.0, s1 = 0.0;
+        if (e0 < kEPB) {
+            long long eg = (long long)(zx0 + e0 % kBX) +
+                           (long long)g.nx * ((zy0 + (e0 / kBX) % kBY) + (long long)g.ny * (zz0 + e0 / (kBX * kBY)));
+            s0 = scale ? scale[eg] : 1.0;
+        }
+        if (e1 < kEPB) {
+            long long eg = (long long)(zx0 + e1 % kBX) +
+                           (long long)g.nx * ((zy0 + (e1 / kBX) % kBY) + (long long)g.ny * (zz0 + e1 / (kBX * kBY)));
+            s1 = scale ? scale[eg] : 1.0;
+        }
+#pragma unroll
+        for (int nt = 0; nt < kNTiles; ++nt) {
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                int n = nt * 8 + 2 * tig + j;
+                if (n < 81) {
+                    if (e0 < kEPB) sy[e0 * 81 + n] = s0 * acc[nt][j];
+                    if (e1 < kEPB) sy[e1 * 81 + n] = s1 * acc[nt][2 + j];
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // node-side sum over the brick's elements, fixed order (z, y, x ascending)
+    double *outb = patch_out + (size_t)b * 3 * kPVol;
+    for (int i = threadIdx.x; i < 3 * kPVol; i += blockDim.x) {
+        int c = i / kPVol, r = i - c * kPVol;
+        int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
+        double sum = 0.0;
+        if (px < ex_n + 2 && py < ey_n + 2 && pz < ez_n + 2) {
+            for (int lz = max(pz - 2, 0); lz <= min(pz, ez_n - 1); ++lz)
+                for (int ly = max(py - 2, 0); ly <= min(py, ey_n - 1); ++ly)
+                    for (int lx = max(px - 2, 0); lx <= min(px, ex_n - 1); ++lx) {
+                        int e = lx + kBX * (ly + kBY * lz);
+                        sum += sy[e * 81 + c * 27 + (px - lx) + 3 * (py - ly) + 9 * (pz - lz)];
+                    }
+        }
+        outb[i] = sum;
+    }
+}
+
+// Bricks containing node j along one direction: the brick min(j / B, nb - 1) and, for the two
+// lowest patch planes of that brick, also the previous one.  Lower brick first.
+__device__ __forceinline__ int node_bricks(int j, int B, int nb, int *bi, int *li) {
+    int i1 = min(j / B, nb - 1);
+    int l1 = j - i1 * B;
+    if (l1 <= 1 && i1 >= 1) {
+        bi[0] = i1 - 1; li[0] = l1 + B;
+        bi[1] = i1; li[1] = l1;
+        return 2;
+    }
+    bi[0] = i1; li[0] = l1;
+    return 1;
+}
+
+// y = sum of brick partials per node, output mask applied; optional partial p'y per CTA.
+__global__ void __launch_bounds__(kVecThreads)
+gather_f64_kernel(Geom g, const double *__restrict__ patch, const double *__restrict__ p,
+                  const uint8_t *__restrict__ mask, int mask_mode, double *__restrict__ y,
+                  double *__restrict__ partials, const PcgState *__restrict__ st) {
+    if (st && st->status != 0) return;
+    double dot = 0.0;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
+         n += (long long)gridDim.x * blockDim.x) {
+        int ix = int(n % g.cx), iy = int((n / g.cx) % g.cy), iz = int(n / ((long long)g.cx * g.cy));
+        int bx[2], lx[2], by[2], ly[2], bz[2], lz[2];
+        int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
+        int nby = node_bricks(iy, kBY, g.nby, by, ly);
+        int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < nbz; ++a)
+            for (int q = 0; q < nby; ++q)
+                for (int w = 0; w < nbx; ++w) {
+                    size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
+                    const double *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
+                    s[0] += pb[0];
+                    s[1] += pb[kPVol];
+                    s[2] += pb[2 * kPVol];
+                }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            long long idx = (long long)c * g.nsc + n;
+            double v = s[c];
+            if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.0;
+            else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
+            y[idx] = v;
+            if (partials) dot += p[idx] * v;
+        }
+    }
+    if (partials) {
+        dot = block_sum(dot);
+        if (threadIdx.x == 0) partials[blockIdx.x] = dot;
+    }
+}
+
+// Jacobi diagonal sum_e s_e K_type(e)[a,a]; elements visited in increasing index so the sum
+// rounds exactly as the assembled CSR entry (rust/src/sparse.rs:166-172, then :70-78).
+__global__ void __launch_bounds__(kVecThreads)
+diagonal_kernel(Geom g, const double *__restrict__ scale, const int *__restrict__ type_id,
+                const double *__restrict__ kdiag, double *__restrict__ d) {
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
+         n += (long long)gridDim.x * blockDim.x) {
+        int ix = int(n % g.cx), iy = int((n / g.cx) % g.cy), iz = int(n / ((long long)g.cx * g.cy));
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int ez = max(iz - 2, 0); ez <= min(iz, g.nz - 1); ++ez)
+            for (int ey = max(iy - 2, 0); ey <= min(iy, g.ny - 1); ++ey)
+                for (int ex = max(ix - 2, 0); ex <= min(ix, g.nx - 1); ++ex) {
+                    long long e = ex + (long long)g.nx * (ey + (long long)g.ny * ez);
+                    double s = scale ? scale[e] : 1.0;
+                    const double *kd = kdiag + (size_t)type_id[e] * 81;
+                    int a = (ix - ex) + 3 * (iy - ey) + 9 * (iz - ez);
+                    s0 = __dadd_rn(s0, __dmul_rn(s, kd[a]));
+                    s1 = __dadd_rn(s1, __dmul_rn(s, kd[27 + a]));
+                    s2 = __dadd_rn(s2, __dmul_rn(s, kd[54 + a]));
+                }
+        d[n] = s0;
+        d[g.nsc + n] = s1;
+        d[2 * g.nsc + n] = s2;
+    }
+}
+
+// ---- PCG vector kernels (rust/src/solver.rs:14-76) -----------------------------------------
+
+__global__ void inv_diag_kernel(long long n, const double *__restrict__ d, double *__restrict__ inv) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        inv[i] = fabs(d[i]) > 1e-12 ? 1.0 / d[i] : 1.0;
+}
+
+// x = 0, r = b, z = D^-1 r, p = z; partials: r'z and b'b
+__global__ void __launch_bounds__(kVecThreads)
+pcg_init_kernel(long long n, const double *__restrict__ b, const double *__restrict__ inv, double *__restrict__ x,
+                double *__restrict__ r, double *__restrict__ p, double *__restrict__ partials) {
+    double rz = 0.0, bb = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double bi = b[i], zi = inv[i] * bi;
+        x[i] = 0.0;
+        r[i] = bi;
+        p[i] = zi;
+        rz += bi * zi;
+        bb += bi * bi;
+    }
+    rz = block_sum(rz);
+    bb = block_sum(bb);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = rz;
+        partials[2 * blockIdx.x + 1] = bb;
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, double tol, long long max_iter) {
+    double rz = 0.0, bb = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        rz += partials[2 * i];
+        bb += partials[2 * i + 1];
+    }
+    rz = block_sum(rz);
+    bb = block_sum(bb);
+    if (threadIdx.x == 0) {
+        st->rz_old = rz;
+        st->norm_b = fmax(sqrt(bb), 1e-16);
+        st->rel_res = 1.0;
+        st->tol = tol;
+        st->iter = 0;
+        st->max_iter = max_iter;
+        st->status = max_iter > 0 ? 0 : kStatMaxIter;
+        st->alpha = st->beta = st->p_ap = 0.0;
+    }
+}
+
+// p'Ap -> alpha, or breakdown (rust/src/solver.rs:41-51)
+__global__ void __launch_bounds__(kVecThreads)
+pcg_alpha_kernel(const double *__restrict__ partials, int np, PcgState *st) {
+    if (st->status != 0) return;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) {
+        st->iter += 1;
+        st->p_ap = s;
+        if (!(s > 0.0)) st->status = isfinite(s) ? kStatBreakdown : kStatNan;
+        else st->alpha = st->rz_old / s;
+    }
+}
+
+// x += alpha p; r -= alpha Ap; partials: r'r and r'z with z = D^-1 r (rust/src/solver.rs:52-66)
+__global__ void __launch_bounds__(kVecThreads)
+pcg_update_kernel(long long n, const double *__restrict__ p, const double *__restrict__ ap,
+                  const double *__restrict__ inv, double *__restrict__ x, double *__restrict__ r,
+                  double *__restrict__ partials, const PcgState *__restrict__ st) {
+    if (st->status != 0) return;
+    const double alpha = st->alpha;
+    double rr = 0.0, rz = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        double ri = r[i] - alpha * ap[i];
+        r[i] = ri;
+        rr += ri * ri;
+        rz += ri * (inv[i] * ri);
+    }
+    rr = block_sum(rr);
+    rz = block_sum(rz);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = rr;
+        partials[2 * blockIdx.x + 1] = rz;
+    }
+}
+
+// relative residual test, then beta (rust/src/solver.rs:56-71)
+__global__ void __launch_bounds__(kVecThreads)
+pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st) {
+    if (st->status != 0) return;
+    double rr = 0.0, rz = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        rr += partials[2 * i];
+        rz += partials[2 * i + 1];
+    }
+    rr = block_sum(rr);
+    rz = block_sum(rz);
+    if (threadIdx.x == 0) {
+        double res = sqrt(rr) / st->norm_b;
+        st->rel_res = res;
+        if (res < st->tol) {
+            st->status = kStatConverged;
+        } else if (!isfinite(res)) {
+            st->status = kStatNan;
+        } else {
+            st->beta = rz / st->rz_old;
+            st->rz_old = rz;
+            if (st->iter >= st->max_iter) st->status = kStatMaxIter;
+        }
+    }
+}
+
+// p = D^-1 r + beta p (rust/src/solver.rs:64-71)
+__global__ void __launch_bounds__(kVecThreads)
+pcg_p_kernel(long long n, const double *__restrict__ r, const double *__restrict__ inv, double *__restrict__ p,
+             const PcgState *__restrict__ st) {
+    if (st->status != 0) return;
+    const double beta = st->beta;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = inv[i] * r[i] + beta * p[i];
+}
+
+// ------------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------------
+
+template <class T>
+static int dev_alloc(T **p, size_t count, const char *what) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    ICC_CUDA(cudaMalloc((void **)p, count * sizeof(T)), what);
+    return ICC_OK;
+}
+
+Op::~Op() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    void *bufs[] = {d_x_in, d_y_out, d_scale, d_kfrag, d_kdiag, d_type_id, d_tile_start, d_tile_type, d_tile_elem,
+                    d_mask, d_patch, d_x, d_r, d_p, d_ap, d_inv, d_b, d_diag, d_partials, d_state};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (h_state) cudaFreeHost(h_state);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+    mixed_release(*this);
+}
+
+int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type_id, const double *scale,
+             const uint8_t *free_mask, int mode) {
+    if (cudaGetDevice(&device) != cudaSuccess) return set_error(ICC_NO_DEVICE, "no CUDA device");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(ICC_NO_DEVICE, "no CUDA device");
+    cudaDeviceProp prop;
+    ICC_CUDA(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major < 10) return set_error(ICC_NO_DEVICE, "device is not sm_100 class (B200 required)");
+    num_sms = prop.multiProcessorCount;
+
+    g.nx = int(s.nel_dir[0]); g.ny = int(s.nel_dir[1]); g.nz = int(s.nel_dir[2]);
+    g.cx = int(s.ncp[0]); g.cy = int(s.ncp[1]); g.cz = int(s.ncp[2]);
+    g.nsc = s.nsc;
+    g.nbx = (g.nx + kBX - 1) / kBX; g.nby = (g.ny + kBY - 1) / kBY; g.nbz = (g.nz + kBZ - 1) / kBZ;
+    g.nbricks = g.nbx * g.nby * g.nbz;
+    nel = s.nel;
+    ndof = s.ndof;
+    ntypes = nt;
+
+    for (int64_t e = 0; e < nel; ++e)
+        if (type_id[e] < 0 || type_id[e] >= nt) return set_error(ICC_BAD_ARG, "type_id out of range");
+
+    ICC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ICC_CUDA(cudaEventCreate(&ev0), "cudaEventCreate");
+    ICC_CUDA(cudaEventCreate(&ev1), "cudaEventCreate");
+
+    // element matrices in DMMA B-fragment order: kfrag[t][ks][nt][lane] = K[n][k] with
+    // k = 4 ks + lane % 4 (trial), n = 8 nt + lane / 4 (test); zero outside 81 x 81.
+    std::vector<double> kf((size_t)nt * kFragPerType, 0.0), kd((size_t)nt * 81);
+    for (int t = 0; t < nt; ++t) {
+        const double *K = ke_types + (size_t)t * 81 * 81;
+        for (int ks = 0; ks < kKSteps; ++ks)
+            for (int ntile = 0; ntile < kNTiles; ++ntile)
+                for (int lane = 0; lane < 32; ++lane) {
+                    int k = 4 * ks + (lane & 3), n = 8 * ntile + (lane >> 2);
+                    kf[(size_t)t * kFragPerType + (ks * kNTiles + ntile) * 32 + lane] =
+                        (k < 81 && n < 81) ? K[n * 81 + k] : 0.0;
+                }
+        for (int a = 0; a < 81; ++a) kd[(size_t)t * 81 + a] = K[a * 81 + a];
+    }
+    host_ktypes.assign(ke_types, ke_types + (size_t)nt * 81 * 81);
+    int rc;
+    if ((rc = dev_alloc(&d_kfrag, kf.size(), "alloc kfrag"))) return rc;
+    if ((rc = dev_alloc(&d_kdiag, kd.size(), "alloc kdiag"))) return rc;
+    ICC_CUDA(cudaMemcpy(d_kfrag, kf.data(), kf.size() * 8, cudaMemcpyHostToDevice), "copy kfrag");
+    ICC_CUDA(cudaMemcpy(d_kdiag, kd.data(), kd.size() * 8, cudaMemcpyHostToDevice), "copy kdiag");
+    if ((rc = dev_alloc(&d_type_id, (size_t)nel, "alloc type_id"))) return rc;
+    ICC_CUDA(cudaMemcpy(d_type_id, type_id, (size_t)nel * 4, cudaMemcpyHostToDevice), "copy type_id");
+    host_type_id.assign(type_id, type_id + nel);
+
+    // brick tile plan: per brick, its elements grouped by type (first-appearance order) and cut
+    // into warp tiles of 16 (255 marks an empty row)
+    std::vector<int> tstart(1, 0), ttype;
+    std::vector<uint8_t> telem;
+    std::vector<int> order, types_seen;
+    for (int b = 0; b < g.nbricks; ++b) {
+        int bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / (g.nbx * g.nby);
+        int x0 = bxi * kBX, y0 = byi * kBY, z0 = bzi * kBZ;
+        types_seen.clear();
+        std::vector<std::vector<int>> groups;
+        for (int lz = 0; lz < kBZ && z0 + lz < g.nz; ++lz)
+            for (int ly = 0; ly < kBY && y0 + ly < g.ny; ++ly)
+                for (int lx = 0; lx < kBX && x0 + lx < g.nx; ++lx) {
+                    int64_t e = (x0 + lx) + (int64_t)g.nx * ((y0 + ly) + (int64_t)g.ny * (z0 + lz));
+                    int t = type_id[e];
+                    size_t gi = std::find(types_seen.begin(), types_seen.end(), t) - types_seen.begin();
+                    if (gi == types_seen.size()) {
+                        types_seen.push_back(t);
+                        groups.emplace_back();
+                    }
+                    groups[gi].push_back(lx + kBX * (ly + kBY * lz));
+                }
+        for (size_t gi = 0; gi < groups.size(); ++gi)
+            for (size_t k = 0; k < groups[gi].size(); k += 16) {
+                ttype.push_back(types_seen[gi]);
+                for (size_t j = 0; j < 16; ++j)
+                    telem.push_back(k + j < groups[gi].size() ? uint8_t(groups[gi][k + j]) : uint8_t(255));
+            }
+        tstart.push_back(int(ttype.size()));
+    }
+    ntiles = int(ttype.size());
+    if ((rc = dev_alloc(&d_tile_start, tstart.size(), "alloc tiles"))) return rc;
+    if ((rc = dev_alloc(&d_tile_type, ttype.size(), "alloc tiles"))) return rc;
+    if ((rc = dev_alloc(&d_tile_elem, telem.size(), "alloc tiles"))) return rc;
+    ICC_CUDA(cudaMemcpy(d_tile_start, tstart.data(), tstart.size() * 4, cudaMemcpyHostToDevice), "copy tiles");
+    ICC_CUDA(cudaMemcpy(d_tile_type, ttype.data(), ttype.size() * 4, cudaMemcpyHostToDevice), "copy tiles");
+    ICC_CUDA(cudaMemcpy(d_tile_elem, telem.data(), telem.size(), cudaMemcpyHostToDevice), "copy tiles");
+
+    if ((rc = dev_alloc(&d_scale, (size_t)nel, "alloc scale"))) return rc;
+    if ((rc = dev_alloc(&d_mask, (size_t)ndof, "alloc mask"))) return rc;
+    if ((rc = dev_alloc(&d_patch, (size_t)g.nbricks * 3 * kPVol, "alloc patch scratch"))) return rc;
+    if ((rc = dev_alloc(&d_x_in, (size_t)ndof, "alloc io"))) return rc;
+    if ((rc = dev_alloc(&d_y_out, (size_t)ndof, "alloc io"))) return rc;
+    vec_blocks = num_sms * 4;
+    if ((rc = dev_alloc(&d_partials, (size_t)vec_blocks * 2, "alloc partials"))) return rc;
+    if ((rc = dev_alloc(&d_state, 1, "alloc state"))) return rc;
+    ICC_CUDA(cudaMallocHost((void **)&h_state, sizeof(PcgState)), "alloc pinned state");
+    ICC_CUDA(cudaFuncSetAttribute(apply_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem),
+             "cudaFuncSetAttribute");
+    if ((rc = set_scale(scale))) return rc;
+    if ((rc = set_mask(free_mask, mode))) return rc;
+    return ICC_OK;
+}
+
+int Op::set_scale(const double *scale) {
+    std::vector<double> ones;
+    const double *src = scale;
+    if (!src) {
+        ones.assign((size_t)nel, 1.0);
+        src = ones.data();
+    }
+    host_scale.assign(src, src + nel);
+    ICC_CUDA(cudaMemcpyAsync(d_scale, src, (size_t)nel * 8, cudaMemcpyHostToDevice, stream), "copy scale");
+    ICC_CUDA(cudaStreamSynchronize(stream), "copy scale");
+    scale_version++;
+    return mixed_on_scale_update(*this);
+}
+
+int Op::set_mask(const uint8_t *free_mask, int mode) {
+    if (mode < 0 || mode > 2) return set_error(ICC_BAD_ARG, "mask_mode must be 0, 1 or 2");
+    mask_mode = (mode != ICC_MASK_NONE && free_mask) ? mode : ICC_MASK_NONE;
+    std::vector<uint8_t> ones;
+    const uint8_t *src = free_mask;
+    if (!src) {
+        ones.assign((size_t)ndof, 1);
+        src = ones.data();
+    }
+    ICC_CUDA(cudaMemcpyAsync(d_mask, src, (size_t)ndof, cudaMemcpyHostToDevice, stream), "copy mask");
+    ICC_CUDA(cudaStreamSynchronize(stream), "copy mask");
+    return ICC_OK;
+}
+
+// Enqueue y = A x on the op's stream (FP64).  partials != null also forms p'y per CTA.
+void Op::enqueue_apply(const double *x, double *y, double *partials, const PcgState *st) {
+    apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
+        g, x, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
+        st);
+    gather_f64_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, x, d_mask, mask_mode, y, partials, st);
+}
+
+int Op::apply_dev(const double *x, double *y) {
+    enqueue_apply(x, y, nullptr, nullptr);
+    ICC_CUDA(cudaGetLastError(), "apply launch");
+    return ICC_OK;
+}
+
+int Op::diagonal_dev(double *d) {
+    diagonal_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(g, d_scale, d_type_id, d_kdiag, d);
+    ICC_CUDA(cudaGetLastError(), "diagonal launch");
+    return ICC_OK;
+}
+
+int Op::ensure_pcg_buffers() {
+    if (d_x) return ICC_OK;
+    int rc;
+    if ((rc = dev_alloc(&d_x, (size_t)ndof, "alloc pcg"))) return rc;
+    if ((rc = dev_alloc(&d_r, (size_t)ndof, "alloc pcg"))) return rc;
+    if ((rc = dev_alloc(&d_p, (size_t)ndof, "alloc pcg"))) return rc;
+    if ((rc = dev_alloc(&d_ap, (size_t)ndof, "alloc pcg"))) return rc;
+    if ((rc = dev_alloc(&d_inv, (size_t)ndof, "alloc pcg"))) return rc;
+    if ((rc = dev_alloc(&d_b, (size_t)ndof, "alloc pcg"))) return rc;
+    if ((rc = dev_alloc(&d_diag, (size_t)ndof, "alloc pcg"))) return rc;
+    return ICC_OK;
+}
+
+// One PCG iteration (rust/src/solver.rs:40-72) as six launches; every kernel returns at once
+// when the state says the solve has finished, so a batch may overrun harmlessly.
+void Op::enqueue_pcg_iteration() {
+    enqueue_apply(d_p, d_ap, d_partials, d_state);
+    pcg_alpha_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
+    pcg_update_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials, d_state);
+    pcg_beta_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
+    pcg_p_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_r, d_inv, d_p, d_state);
+}
+
+int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_iter, int check_every, double *x,
+                 int64_t *iters, double *rel_res) {
+    int rc;
+    if ((rc = ensure_pcg_buffers())) return rc;
+    int64_t launches = 3;
+    if (!diag) {
+        if ((rc = diagonal_dev(d_diag))) return rc;
+        diag = d_diag;
+        launches += 1;
+    }
+    inv_diag_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, diag, d_inv);
+    pcg_init_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, b, d_inv, d_x, d_r, d_p, d_partials);
+    pcg_init_finalize<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state, tol, max_iter);
+    ICC_CUDA(cudaGetLastError(), "pcg init");
+    if (check_every <= 0) check_every = 32;
+    if (!graph_exec || graph_batch != check_every) {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        cudaGraph_t graph;
+        ICC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        for (int i = 0; i < check_every; ++i) enqueue_pcg_iteration();
+        ICC_CUDA(cudaStreamEndCapture(stream, &graph), "end capture");
+        cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        ICC_CUDA(e, "graph instantiate");
+        graph_batch = check_every;
+    }
+    int64_t launched = 0;
+    for (;;) {
+        ICC_CUDA(cudaMemcpyAsync(h_state, d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
+        ICC_CUDA(cudaStreamSynchronize(stream), "pcg sync");
+        if (h_state->status != 0) break;
+        if (launched > max_iter + 2 * int64_t(check_every))
+            return set_error(ICC_TIMEOUT, "pcg: device state did not reach a stop condition");
+        ICC_CUDA(cudaGraphLaunch(graph_exec, stream), "graph launch");
+        launched += check_every;
+        launches += 6 * int64_t(check_every);
+    }
+    ICC_CUDA(cudaMemcpyAsync(x, d_x, (size_t)ndof * 8, cudaMemcpyDeviceToDevice, stream), "copy x");
+    *iters = h_state->iter;
+    *rel_res = h_state->rel_res;
+    last_info.iterations = h_state->iter;
+    last_info.outer_iterations = 0;
+    last_info.rel_res = h_state->rel_res;
+    last_info.fp64_applies = h_state->iter;
+    last_info.mixed_applies = 0;
+    last_info.kernel_launches = launches;
+    switch (h_state->status) {
+        case kStatConverged: return ICC_OK;
+        case kStatBreakdown: return ICC_BREAKDOWN;
+        case kStatMaxIter: return ICC_NOT_CONVERGED;
+        default: return set_error(ICC_NAN, "pcg: non-finite reduction (NaN input or non-SPD operator)");
+    }
+}
+
+}  // namespace icc
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+using icc::set_error;
+
+struct icc_op {
+    icc::Op op;
+};
+
+extern "C" {
+
+const char *icc_last_error(void) { return icc::g_last_error.c_str(); }
+
+int icc_op_create(const icc_space *sp, const double *ke_types, int32_t ntypes, const int32_t *type_id,
+                  const double *scale, const uint8_t *free_mask, int32_t mask_mode, icc_op **out) {
+    if (!sp || !ke_types || !type_id || !out || ntypes <= 0)
+        return set_error(ICC_BAD_ARG, "icc_op_create: null argument or ntypes <= 0");
+    *out = nullptr;
+    auto *h = new (std::nothrow) icc_op();
+    if (!h) return set_error(ICC_OUT_OF_MEMORY, "icc_op_create: out of host memory");
+    int rc = h->op.init(sp->s, ke_types, ntypes, type_id, scale, free_mask, mask_mode);
+    if (rc != ICC_OK) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return ICC_OK;
+}
+
+int icc_op_create_lame(const icc_space *sp, double lambda, double mu, const double *scale,
+                       const uint8_t *free_mask, int32_t mask_mode, icc_op **out) {
+    if (!sp || !out) return set_error(ICC_BAD_ARG, "icc_op_create_lame: null argument");
+    std::vector<double> ke;
+    std::vector<int32_t> tid;
+    std::vector<std::array<int, 3>> combos;
+    sp->s.element_types(lambda, mu, ke, tid, combos);
+    return icc_op_create(sp, ke.data(), int32_t(combos.size()), tid.data(), scale, free_mask, mask_mode, out);
+}
+
+void icc_op_destroy(icc_op *op) {
+    if (!op) return;
+    cudaSetDevice(op->op.device);
+    delete op;
+}
+
+int icc_op_update_scale(icc_op *op, const double *scale) {
+    if (!op) return set_error(ICC_BAD_ARG, "icc_op_update_scale: null op");
+    cudaSetDevice(op->op.device);
+    return op->op.set_scale(scale);
+}
+
+int icc_op_update_mask(icc_op *op, const uint8_t *free_mask, int32_t mask_mode) {
+    if (!op) return set_error(ICC_BAD_ARG, "icc_op_update_mask: null op");
+    cudaSetDevice(op->op.device);
+    return op->op.set_mask(free_mask, mask_mode);
+}
+
+void *icc_op_stream(icc_op *op) { return op ? (void *)op->op.stream : nullptr; }
+
+int icc_op_apply_dev(icc_op *op, const double *x, double *y, int64_t n) {
+    if (!op || !x || !y) return set_error(ICC_BAD_ARG, "icc_op_apply_dev: null argument");
+    if (n != op->op.ndof) return set_error(ICC_BAD_ARG, "icc_op_apply_dev: n != ndof");
+    cudaSetDevice(op->op.device);
+    return op->op.apply_dev(x, y);
+}
+
+int icc_op_apply(icc_op *op, const double *x, double *y, int64_t n) {
+    if (!op || !x || !y) return set_error(ICC_BAD_ARG, "icc_op_apply: null argument");
+    icc::Op &o = op->op;
+    if (n != o.ndof) return set_error(ICC_BAD_ARG, "icc_op_apply: n != ndof");
+    cudaSetDevice(o.device);
+    ICC_CUDA(cudaMemcpyAsync(o.d_x_in, x, (size_t)n * 8, cudaMemcpyHostToDevice, o.stream), "apply h2d");
+    int rc = o.apply_dev(o.d_x_in, o.d_y_out);
+    if (rc) return rc;
+    ICC_CUDA(cudaMemcpyAsync(y, o.d_y_out, (size_t)n * 8, cudaMemcpyDeviceToHost, o.stream), "apply d2h");
+    ICC_CUDA(cudaStreamSynchronize(o.stream), "apply sync");
+    return ICC_OK;
+}
+
+int icc_op_diagonal(icc_op *op, double *d, int64_t n) {
+    if (!op || !d) return set_error(ICC_BAD_ARG, "icc_op_diagonal: null argument");
+    icc::Op &o = op->op;
+    if (n != o.ndof) return set_error(ICC_BAD_ARG, "icc_op_diagonal: n != ndof");
+    cudaSetDevice(o.device);
+    int rc = o.diagonal_dev(o.d_y_out);
+    if (rc) return rc;
+    ICC_CUDA(cudaMemcpyAsync(d, o.d_y_out, (size_t)n * 8, cudaMemcpyDeviceToHost, o.stream), "diag d2h");
+    ICC_CUDA(cudaStreamSynchronize(o.stream), "diag sync");
+    return ICC_OK;
+}
+
+static int solve_common(icc_op *op, const double *b_dev, const double *diag_dev, int64_t n, double tol,
+                        int64_t max_iter, const icc_solve_opts *opts, double *x_dev, int64_t *iters, double *rel_res) {
+    icc::Op &o = op->op;
+    if (n != o.ndof) return set_error(ICC_BAD_ARG, "icc_pcg_solve: n != ndof");
+    if (max_iter < 0 || !(tol >= 0.0)) return set_error(ICC_BAD_ARG, "icc_pcg_solve: bad tol or max_iter");
+    icc_solve_opts def = {ICC_FP64, 32, 0.0, 0, 0};
+    const icc_solve_opts *op_ = opts ? opts : &def;
+    int64_t it = 0;
+    double rr = 1.0;
+    cudaEventRecord(o.ev0, o.stream);
+    int rc;
+    if (op_->precision == ICC_FP64) {
+        rc = o.pcg_fp64(b_dev, diag_dev, tol, max_iter, op_->check_every, x_dev, &it, &rr);
+    } else if (op_->precision == ICC_MIXED) {
+        rc = icc::mixed_solve(o, b_dev, diag_dev, tol, max_iter, *op_, x_dev, &it, &rr);
+    } else {
+        return set_error(ICC_BAD_ARG, "icc_pcg_solve: unknown precision");
+    }
+    cudaEventRecord(o.ev1, o.stream);
+    cudaEventSynchronize(o.ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, o.ev0, o.ev1);
+    o.last_info.device_ms = ms;
+    if (iters) *iters = it;
+    if (rel_res) *rel_res = rr;
+    return rc;
+}
+
+int icc_pcg_solve_dev(icc_op *op, const double *b_dev, const double *diag_dev, int64_t n, double tol,
+                      int64_t max_iter, const icc_solve_opts *opts, double *x_dev, int64_t *iters, double *rel_res) {
+    if (!op || !b_dev || !x_dev) return set_error(ICC_BAD_ARG, "icc_pcg_solve_dev: null argument");
+    cudaSetDevice(op->op.device);
+    int rc = solve_common(op, b_dev, diag_dev, n, tol, max_iter, opts, x_dev, iters, rel_res);
+    cudaError_t e = cudaStreamSynchronize(op->op.stream);
+    if (e != cudaSuccess && rc >= 0) return icc::set_error(ICC_CUDA_ERROR, cudaGetErrorString(e));
+    return rc;
+}
+
+int icc_pcg_solve(icc_op *op, const double *b, const double *diag, int64_t n, double tol, int64_t max_iter,
+                  const icc_solve_opts *opts, double *x, int64_t *iters, double *rel_res) {
+    if (!op || !b || !x) return set_error(ICC_BAD_ARG, "icc_pcg_solve: null argument");
+    icc::Op &o = op->op;
+    if (n != o.ndof) return set_error(ICC_BAD_ARG, "icc_pcg_solve: n != ndof");
+    cudaSetDevice(o.device);
+    int rc = o.ensure_pcg_buffers();
+    if (rc) return rc;
+    ICC_CUDA(cudaMemcpyAsync(o.d_b, b, (size_t)n * 8, cudaMemcpyHostToDevice, o.stream), "solve h2d");
+    if (diag) ICC_CUDA(cudaMemcpyAsync(o.d_diag, diag, (size_t)n * 8, cudaMemcpyHostToDevice, o.stream), "solve h2d");
+    rc = solve_common(op, o.d_b, diag ? o.d_diag : nullptr, n, tol, max_iter, opts, o.d_y_out, iters, rel_res);
+    if (rc < 0) return rc;
+    ICC_CUDA(cudaMemcpyAsync(x, o.d_y_out, (size_t)n * 8, cudaMemcpyDeviceToHost, o.stream), "solve d2h");
+    ICC_CUDA(cudaStreamSynchronize(o.stream), "solve sync");
+    return rc;
+}
+
+int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t reps, double *contract_ms,
+                         double *gather_ms) {
+    if (!op || !x_dev || !y_dev || reps <= 0) return set_error(ICC_BAD_ARG, "icc_op_profile_apply: bad argument");
+    icc::Op &o = op->op;
+    cudaSetDevice(o.device);
+    std::vector<cudaEvent_t> ev(3 * size_t(reps));
+    for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(ev[3 * r], o.stream);
+        icc::apply_f64_kernel<<<o.g.nbricks, icc::kApplyThreads, icc::kApplySmem, o.stream>>>(
+            o.g, x_dev, o.d_mask, o.mask_mode != ICC_MASK_NONE, o.d_scale, o.d_kfrag, o.d_tile_start, o.d_tile_type,
+            o.d_tile_elem, o.d_patch, nullptr);
+        cudaEventRecord(ev[3 * r + 1], o.stream);
+        icc::gather_f64_kernel<<<o.vec_blocks, icc::kVecThreads, 0, o.stream>>>(o.g, o.d_patch, x_dev, o.d_mask,
+                                                                                o.mask_mode, y_dev, nullptr, nullptr);
+        cudaEventRecord(ev[3 * r + 2], o.stream);
+    }
+    cudaError_t e = cudaEventSynchronize(ev.back());
+    double a = 0.0, g = 0.0;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        float t1 = 0.f, t2 = 0.f;
+        cudaEventElapsedTime(&t1, ev[3 * r], ev[3 * r + 1]);
+        cudaEventElapsedTime(&t2, ev[3 * r + 1], ev[3 * r + 2]);
+        a += t1;
+        g += t2;
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    ICC_CUDA(e, "profile apply");
+    if (contract_ms) *contract_ms = a / reps;
+    if (gather_ms) *gather_ms = g / reps;
+    return ICC_OK;
+}
+
+int icc_op_last_solve_info(const icc_op *op, icc_solve_info *info) {
+    if (!op || !info) return set_error(ICC_BAD_ARG, "icc_op_last_solve_info: null argument");
+    *info = op->op.last_info;
+    return ICC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,198 @@
+"""Synthetic inputs of the benchmark configurations (numpy only; seeded PCG64).
+
+* cantilever(nel, smooth):  the SIMP cantilever on the box [0,2] x [0,1] x [0,1]: E0 = 1,
+  E_min = 1e-9, nu = 0.3, SIMP penalty 3, densities i.i.d. U[0.01, 1] (optionally smoothed by a
+  3x3x3 box filter with clamped indices), control points with ix = 0 clamped in all components,
+  and the consistent load of a unit total downward traction spread uniformly over the face
+  x = 2.  24x16x12 elements is the CPU-runnable case, 128x64x64 the at-scale case.
+* cylinders(n):  the immersed case: unit cube minus three orthogonal through-cylinders of
+  radius 0.25, per-cell volume fraction by 8^3 midpoint sub-sampling after corner
+  classification (the rule of rust/src/immersed.rs:89-155 with an exact inside test), alpha <
+  1e-3 inactive, alpha floored at 1e-6, clamped at z = 0, pressure 1 on the z = 1 face.
+
+The element scale follows the reference: s_e = E_min + rho^p (E0 - E_min) (rust/src/topopt_iga.rs:132
+with E0 folded into the Lame parameters), times alpha for immersed cells
+(rust/src/topopt_immersed.rs:166).
+"""
+from dataclasses import dataclass
+
+import numpy as np
+
+E0, EMIN, NU, PENAL = 1.0, 1e-9, 0.3, 3.0
+
+
+@dataclass
+class Problem:
+    name: str
+    bounds: np.ndarray      # [3, 2]
+    nel: tuple              # (nx, ny, nz)
+    scale: np.ndarray       # [nel] float64, s_e
+    free_mask: np.ndarray   # [ndof] uint8
+    force: np.ndarray       # [ndof] float64
+    density: np.ndarray     # [nel]
+    alpha: np.ndarray = None  # [nel] volume fraction (immersed)
+
+    @property
+    def ncp(self):
+        return tuple(n + 2 for n in self.nel)
+
+    @property
+    def ndof(self):
+        cx, cy, cz = self.ncp
+        return 3 * cx * cy * cz
+
+
+def open_knot_integrals(nel, length):
+    """int_0^L N_i for the p = 2 open uniform knot vector: L (k[i+3] - k[i]) / 3."""
+    kn = np.concatenate([[0.0, 0.0, 0.0], np.arange(1, nel) / nel, [1.0, 1.0, 1.0]])
+    return length * (kn[3:] - kn[:-3]) / 3.0
+
+
+def box_filter_clamped(r):
+    """3x3x3 mean with clamped (edge-replicated) indices; r has shape (nz, ny, nx)."""
+    p = np.pad(r, 1, mode="edge")
+    nz, ny, nx = r.shape
+    acc = np.zeros_like(r)
+    for dz in range(3):
+        for dy in range(3):
+            for dx in range(3):
+                acc += p[dz:dz + nz, dy:dy + ny, dx:dx + nx]
+    return acc / 27.0
+
+
+def cantilever(nel=(24, 16, 12), smooth=False, seed=0, name=None):
+    nx, ny, nz = nel
+    bounds = np.array([[0.0, 2.0], [0.0, 1.0], [0.0, 1.0]])
+    rng = np.random.default_rng(seed)
+    rho = rng.uniform(0.01, 1.0, size=(nz, ny, nx))
+    if smooth:
+        rho = box_filter_clamped(rho)
+    rho = rho.reshape(-1)
+    scale = EMIN + rho ** PENAL * (E0 - EMIN)
+    cx, cy, cz = nx + 2, ny + 2, nz + 2
+    nsc = cx * cy * cz
+    ix = np.arange(nsc) % cx
+    free = np.ones(3 * nsc, dtype=np.uint8)
+    for c in range(3):
+        free[c * nsc:(c + 1) * nsc][ix == 0] = 0
+    wy = open_knot_integrals(ny, bounds[1, 1] - bounds[1, 0])
+    wz = open_knot_integrals(nz, bounds[2, 1] - bounds[2, 0])
+    area = (bounds[1, 1] - bounds[1, 0]) * (bounds[2, 1] - bounds[2, 0])
+    force = np.zeros(3 * nsc)
+    face = np.zeros((cz, cy))
+    face[:, :] = -(wz[:, None] * wy[None, :]) / area
+    fz = force[2 * nsc:3 * nsc].reshape(cz, cy, cx)
+    fz[:, :, cx - 1] = face
+    return Problem(name or f"cantilever_{nx}x{ny}x{nz}", bounds, (nx, ny, nz), scale, free, force, rho)
+
+
+def _cyl_inside(x, y, z, r):
+    inside = (x >= 0) & (x <= 1) & (y >= 0) & (y <= 1) & (z >= 0) & (z <= 1)
+    x, y, z = x - 0.5, y - 0.5, z - 0.5
+    r2 = r * r
+    hole = (y * y + z * z < r2) | (x * x + z * z < r2) | (x * x + y * y < r2)
+    return inside & ~hole
+
+
+def cylinder_fractions(n, sub=8, radius=0.25):
+    """Per-cell volume fraction and status (1 inside, 0 outside, -1 cut) on an n^3 grid of [0,1]^3."""
+    xs = np.linspace(0.0, 1.0, n + 1)
+    xs[-1] = 1.0
+    Z, Y, X = np.meshgrid(xs, xs, xs, indexing="ij")
+    ins = _cyl_inside(X, Y, Z, radius).astype(np.int32)
+    cnt = sum(ins[dz:dz + n, dy:dy + n, dx:dx + n] for dz in (0, 1) for dy in (0, 1) for dx in (0, 1))
+    status = np.where(cnt == 8, 1, np.where(cnt == 0, 0, -1)).astype(np.int8)
+    w = np.where(status == 1, 1.0, 0.0)
+    h = 1.0 / n
+    cut = np.argwhere(status == -1)
+    off = (np.arange(sub) + 0.5) * (h / sub)
+    for k, j, i in cut:
+        zz, yy, xx = np.meshgrid(k * h + off, j * h + off, i * h + off, indexing="ij")
+        w[k, j, i] = _cyl_inside(xx, yy, zz, radius).sum() / float(sub ** 3)
+    return w.reshape(-1), status.reshape(-1)
+
+
+def cylinders(n=96, sub=8, radius=0.25, name=None):
+    bounds = np.array([[0.0, 1.0], [0.0, 1.0], [0.0, 1.0]])
+    alpha, _ = cylinder_fractions(n, sub, radius)
+    alpha = alpha.astype(np.float32).astype(np.float64)   # stored in FP32
+    active = alpha >= 1e-3
+    a = np.where(active, np.maximum(alpha, 1e-6), 0.0)
+    scale = (EMIN + 1.0 * (E0 - EMIN)) * a               # density 1
+    cx = cy = cz = n + 2
+    nsc = cx * cy * cz
+    # control points touched by no active cell carry no stiffness: mask them out
+    act = active.reshape(n, n, n)
+    touched = np.zeros((cz, cy, cx), dtype=bool)
+    for dz in range(3):
+        for dy in range(3):
+            for dx in range(3):
+                touched[dz:dz + n, dy:dy + n, dx:dx + n] |= act
+    iz = np.arange(nsc) // (cx * cy)
+    free_sc = touched.reshape(-1) & (iz != 0)
+    free = np.tile(free_sc.astype(np.uint8), 3)
+    # consistent pressure load on the solid part of z = 1: -int_{top face, solid} N_i dA
+    w1 = open_knot_integrals(n, 1.0)
+    top = alpha.reshape(n, n, n)[n - 1] > 0  # cells of the top layer with material
+    # per-cell exact integral of N_ix N_iy over a cell: use 3-point Gauss per cell
+    force = np.zeros(3 * nsc)
+    fz = force[2 * nsc:].reshape(cz, cy, cx)
+    gx, gw = np.polynomial.legendre.leggauss(3)
+    kn = np.concatenate([[0.0, 0.0, 0.0], np.arange(1, n) / n, [1.0, 1.0, 1.0]])
+    def basis(e, t):
+        # the three nonzero quadratic B-splines on element e at local t in [0,1]
+        x = (e + t) / n
+        vals = np.zeros(3)
+        for r in range(3):
+            i = e + r
+            vals[r] = _bspline2(kn, i, x)
+        return vals
+    sub_pts = 8
+    soff = (np.arange(sub_pts) + 0.5) / sub_pts
+    for j in range(n):
+        for i in range(n):
+            if not top[j, i]:
+                continue
+            # fraction of the top face of the cell covered by solid, by sub-sampling at z = 1
+            xs_ = (i + soff) / n
+            ys_ = (j + soff) / n
+            YY, XX = np.meshgrid(ys_, xs_, indexing="ij")
+            solid = _cyl_inside(XX, YY, np.full_like(XX, 1.0 - 1e-12), radius)
+            if not solid.any():
+                continue
+            bx = np.stack([basis(i, t) for t in soff])  # [sub, 3]
+            by = np.stack([basis(j, t) for t in soff])
+            wgt = solid.astype(float) * (1.0 / n / sub_pts) ** 2
+            contrib = np.einsum("yx,ya,xb->ab", wgt, by, bx)  # [3 (y), 3 (x)]
+            fz[cz - 1, j:j + 3, i:i + 3] -= contrib
+    del w1, gx, gw
+    rho = np.ones(n ** 3)
+    return Problem(name or f"cylinders_{n}", bounds, (n, n, n), scale, free, force * free, rho, alpha)
+
+
+def _bspline2(kn, i, x):
+    """Quadratic B-spline N_i(x) on knots kn (Cox-de Boor), right end included in the last span."""
+    def n0(j, x):
+        if kn[j] <= x < kn[j + 1]:
+            return 1.0
+        if x == kn[-1] and kn[j] < kn[j + 1] == kn[-1]:
+            return 1.0
+        return 0.0
+
+    def nk(j, k, x):
+        if k == 0:
+            return n0(j, x)
+        a = 0.0
+        d1 = kn[j + k] - kn[j]
+        if d1 > 0:
+            a += (x - kn[j]) / d1 * nk(j, k - 1, x)
+        d2 = kn[j + k + 1] - kn[j + 1]
+        if d2 > 0:
+            a += (kn[j + k + 1] - x) / d2 * nk(j + 1, k - 1, x)
+        return a
+
+    return nk(i, 2, x)
+
+
+def rhs_masked(p: Problem):
+    return np.where(p.free_mask > 0, p.force, 0.0)

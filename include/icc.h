@@ -1,0 +1,141 @@
+/*
+ * icc.h -- C ABI of the B200 matrix-free B-spline elasticity operator and Jacobi-PCG solver.
+ *
+ * The operator is y = sum_e s_e K_type(e) u_e on a uniform quadratic (p = 2) tensor-product
+ * B-spline grid over an axis-aligned box, with the reference's numbering:
+ *   control point g = ix + ncx*(iy + ncy*iz)            (rust/src/iga/space.rs:133-147)
+ *   DOF           c*ndof_sc + g (component-blocked)     (rust/src/iga/space.rs:148-155)
+ *   element-local a = ax + 3*(ay + 3*az), DOF c*27 + a  (rust/src/iga/space.rs:4-9)
+ *   K_type rows = test, columns = trial, row-major 81x81 (rust/src/iga/elasticity.rs:14-26)
+ *
+ * All entry points return an int status (ICC_OK = 0) and never abort.  Host arrays are
+ * borrowed for the duration of the call; device state is owned by the handle.  A handle is
+ * bound to the CUDA device that was current when it was created, and runs its work on its own
+ * stream.  Handles are not thread-safe.
+ */
+#ifndef ICC_H
+#define ICC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define ICC_OK 0
+#define ICC_NOT_CONVERGED 1   /* PCG hit max_iter before the tolerance */
+#define ICC_BREAKDOWN 2       /* p'Ap <= 0 (rust/src/solver.rs:45-49): returns the current iterate */
+#define ICC_BAD_ARG (-1)
+#define ICC_CUDA_ERROR (-2)
+#define ICC_TIMEOUT (-3)
+#define ICC_NO_DEVICE (-4)
+#define ICC_OUT_OF_MEMORY (-5)
+#define ICC_NAN (-6)          /* a reduction produced NaN/Inf (NaN input or a non-SPD operator) */
+
+/* ---- mask modes (the closures the reference wraps around CsrMatrix::matvec) ------------- */
+#define ICC_MASK_NONE 0       /* y = K x                                   (rust/src/sparse.rs:60-68) */
+#define ICC_MASK_ZERO 1       /* y = m.*K(m.*x)                   (rust/src/topopt_iga.rs:151-159,
+                                                                   rust/src/immersed.rs:558-566) */
+#define ICC_MASK_IDENTITY 2   /* y = K(m.*x) on free rows, y = x on fixed (rust/tests/iga_kernel.rs:101-107) */
+
+/* ---- precision forms of the solve ---------------------------------------------------------- */
+#define ICC_FP64 0            /* all-FP64 apply, vectors and reductions */
+#define ICC_MIXED 1           /* FP64 iterative refinement around an inner FP32 PCG whose apply runs
+                                 on the tensor cores as a 3-term split-TF32 product */
+
+typedef struct icc_space icc_space;
+typedef struct icc_op icc_op;
+
+typedef struct icc_solve_opts {
+    int32_t precision;        /* ICC_FP64 or ICC_MIXED */
+    int32_t check_every;      /* PCG iterations between convergence checks on the host (0: 32) */
+    double inner_tol;         /* ICC_MIXED: inner relative residual per refinement step (0: 1e-3) */
+    int32_t max_outer;        /* ICC_MIXED: maximum refinement steps (0: 60) */
+    int32_t reserved;
+} icc_solve_opts;
+
+typedef struct icc_solve_info {
+    int64_t iterations;       /* PCG iterations (ICC_FP64) or inner iterations summed (ICC_MIXED) */
+    int64_t outer_iterations; /* refinement steps (ICC_MIXED), 0 otherwise */
+    double rel_res;           /* final relative residual (recurrence residual for ICC_FP64, as in
+                                 rust/src/solver.rs:56-58; true FP64 residual for ICC_MIXED) */
+    double device_ms;         /* device time of the solve (CUDA events on the handle's stream) */
+    int64_t fp64_applies;     /* FP64 operator applications */
+    int64_t mixed_applies;    /* tensor-core (split-TF32) operator applications */
+    int64_t kernel_launches;  /* kernels this library launched for the solve */
+} icc_solve_info;
+
+/* Text of the last error on this thread ("" if none). */
+const char *icc_last_error(void);
+
+/* ---- space (rust/src/iga/space.rs:107 SpaceBox::new) --------------------------------------
+ * bounds = {x0, x1, y0, y1, z0, z1}; nsub = elements per direction; degree must be 2 and the
+ * box 3-D (the hot path); open uniform knots of maximal regularity (rust/src/iga/quadrature.rs:51). */
+int icc_space_create(const double bounds[6], const int64_t nsub[3], int32_t degree, icc_space **out);
+void icc_space_destroy(icc_space *sp);
+/* ndof, nel, control points per direction, elements per direction */
+int icc_space_dims(const icc_space *sp, int64_t *ndof, int64_t *nel, int64_t ndof_dir[3], int64_t nel_dir[3]);
+/* SpaceBox::connectivity (rust/src/iga/space.rs:148-155): conn[e*81 + c*27 + a] */
+int icc_space_connectivity(const icc_space *sp, int64_t *conn);
+
+/* ---- element matrices ----------------------------------------------------------------------- */
+/* rust/src/iga/elasticity.rs:173-177 lame */
+void icc_lame(double young, double poisson, double *lambda, double *mu);
+/* rust/src/iga/elasticity.rs:30-150 elasticity_element_matrices: writes ntypes row-major 81x81
+ * matrices (capacity max_types) and the type of every element, type ids in order of first
+ * appearance exactly as the reference groups them. */
+int icc_element_matrices(const icc_space *sp, double lambda, double mu, double *ke_types,
+                         int32_t max_types, int32_t *type_id, int32_t *ntypes);
+
+/* ---- operator --------------------------------------------------------------------------------
+ * Replaces AssemblyPattern::assemble + CsrMatrix (rust/src/sparse.rs:128-175, :60-78) by a
+ * matrix-free device operator.  ke_types[ntypes*81*81], type_id[nel], scale[nel] (s_e, NULL = 1),
+ * free_mask[ndof] (NULL = all free; ignored for ICC_MASK_NONE). */
+int icc_op_create(const icc_space *sp, const double *ke_types, int32_t ntypes, const int32_t *type_id,
+                  const double *scale, const uint8_t *free_mask, int32_t mask_mode, icc_op **out);
+/* Convenience: element matrices from (lambda, mu) built on the host as icc_element_matrices does. */
+int icc_op_create_lame(const icc_space *sp, double lambda, double mu, const double *scale,
+                       const uint8_t *free_mask, int32_t mask_mode, icc_op **out);
+void icc_op_destroy(icc_op *op);
+/* Per-design-iteration rescale: replaces AssemblyPattern::assemble(|e| .., &scale)
+ * (rust/src/sparse.rs:160, called from rust/src/topopt_iga.rs:131-134). */
+int icc_op_update_scale(icc_op *op, const double *scale);
+int icc_op_update_mask(icc_op *op, const uint8_t *free_mask, int32_t mask_mode);
+/* y = A x with A the masked operator (host arrays of length n = ndof); mirrors the closure
+ * around CsrMatrix::matvec (rust/src/sparse.rs:60-68). */
+int icc_op_apply(icc_op *op, const double *x, double *y, int64_t n);
+/* Same on device arrays, enqueued on the handle's stream (see icc_op_stream). */
+int icc_op_apply_dev(icc_op *op, const double *x_dev, double *y_dev, int64_t n);
+/* CsrMatrix::diagonal (rust/src/sparse.rs:70-78) of the unmasked operator: sum_e s_e K[a,a],
+ * accumulated in element order, bit-identical to the assembled CSR diagonal. */
+int icc_op_diagonal(icc_op *op, double *d, int64_t n);
+/* cudaStream_t of the handle (as void*), for callers that time or order device work. */
+void *icc_op_stream(icc_op *op);
+
+/* ---- solve: PcgSolver::new(max_iter, tol).solve(n, b, diag, closure) (rust/src/solver.rs:9-76)
+ * x starts at 0, Jacobi preconditioner inv_diag = |d| > 1e-12 ? 1/d : 1, stop when
+ * ||r||/max(||b||, 1e-16) < tol, break when p'Ap <= 0.  diag NULL = the operator's own diagonal.
+ * Returns ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN or an error; x, iters and rel_res are
+ * written in every non-error case (as the reference returns its current iterate). */
+int icc_pcg_solve(icc_op *op, const double *b, const double *diag, int64_t n, double tol, int64_t max_iter,
+                  const icc_solve_opts *opts, double *x, int64_t *iters, double *rel_res);
+/* Same on device arrays (b_dev, diag_dev may be NULL for the operator diagonal). */
+int icc_pcg_solve_dev(icc_op *op, const double *b_dev, const double *diag_dev, int64_t n, double tol,
+                      int64_t max_iter, const icc_solve_opts *opts, double *x_dev, int64_t *iters,
+                      double *rel_res);
+/* Details of the last solve on this handle. */
+int icc_op_last_solve_info(const icc_op *op, icc_solve_info *info);
+
+/* ---- diagnostics (no reference counterpart) -------------------------------------------------
+ * Times `reps` FP64 applies of x_dev on the handle's stream with CUDA events around each of the
+ * two kernels of an apply (the element-brick contraction and the node-side sum); returns the
+ * mean milliseconds of each.  Used by the benchmark for the roofline figure. */
+int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t reps, double *contract_ms,
+                         double *gather_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICC_H */
