@@ -37,6 +37,7 @@ SEED = 2026
 WORKLOADS = {
     "cantilever128": dict(nel=(128, 64, 64), smooth=True),
     "cantilever24": dict(nel=(24, 16, 12), smooth=False),
+    "cantilever256": dict(nel=(256, 128, 128), smooth=True),
 }
 
 
@@ -51,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-solution", action="store_true", help="skip the tight FP64 error reference")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only run warmup + steps operator applies (for profiler captures)")
     return ap.parse_args()
 
 
@@ -167,7 +170,7 @@ def run_reference(args):
     O.build()
     wl = WORKLOADS[args.workload]
     prob = W.cantilever(wl["nel"], smooth=wl["smooth"], seed=SEED)
-    per_step = max(2.0, min(60.0, args.cpu_seconds))
+    per_step = max(2.0, min(10.0, args.cpu_seconds))
     vals = []
     for i in range(args.warmup + args.steps):
         s = cpu_sample(prob, per_step, O)
@@ -217,6 +220,25 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+
+    if args.kernel_only:
+        y_dev = torch.empty_like(x_dev)
+        p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev)
+        for _ in range(args.warmup):
+            op.matvec_dev(p_dev.data_ptr(), y_dev.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        for _ in range(args.steps):
+            op.matvec_dev(p_dev.data_ptr(), y_dev.data_ptr())
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        if rank == 0:
+            print(json.dumps({"kernel_only": True, "workload": prob.name, "ndof": n,
+                              "ms_per_apply": e0.elapsed_time(e1) / args.steps}), flush=True)
+        return
 
     for _ in range(args.warmup):
         solver.solve_dev(n, b_dev.data_ptr(), 0, x_dev.data_ptr(), op)
