@@ -40,7 +40,8 @@ FP64, MIXED = 0, 1
 EXPORTED = [
     "icc_last_error", "icc_space_create", "icc_space_destroy", "icc_space_dims", "icc_space_connectivity",
     "icc_lame", "icc_element_matrices", "icc_op_create", "icc_op_create_lame", "icc_op_destroy",
-    "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_diagonal",
+    "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_apply_f32",
+    "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
 ]
 
@@ -66,6 +67,7 @@ _lib = None
 f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 
 def lib():
@@ -93,6 +95,8 @@ def lib():
     L.icc_op_update_mask.argtypes = [vp, vp, i32]
     L.icc_op_apply.argtypes = [vp, f64p, f64p, i64]
     L.icc_op_apply_dev.argtypes = [vp, vp, vp, i64]
+    L.icc_op_apply_f32.argtypes = [vp, f32p, f32p, i64]
+    L.icc_op_apply_f32_dev.argtypes = [vp, vp, vp, i64]
     L.icc_op_diagonal.argtypes = [vp, f64p, i64]
     L.icc_op_stream.argtypes = [vp]
     L.icc_op_stream.restype = vp
@@ -213,6 +217,15 @@ class MatrixFreeOperator:
         y = np.zeros(self.n)
         _check(lib().icc_op_apply(self._h, np.ascontiguousarray(x, dtype=np.float64), y, self.n))
         return y
+
+    def matvec_f32(self, x):
+        """FP32 tensor-core apply (the mixed form's inner operator)."""
+        y = np.zeros(self.n, dtype=np.float32)
+        _check(lib().icc_op_apply_f32(self._h, np.ascontiguousarray(x, dtype=np.float32), y, self.n))
+        return y
+
+    def matvec_f32_dev(self, x_ptr, y_ptr):
+        _check(lib().icc_op_apply_f32_dev(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), self.n))
 
     def matvec_dev(self, x_ptr, y_ptr):
         """Device pointers (e.g. torch tensor .data_ptr()); enqueued on the operator's stream."""

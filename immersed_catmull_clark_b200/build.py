@@ -11,7 +11,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libicc.so")
 SOURCES = ["icc_op.cu", "icc_mixed.cu", "icc_space.cpp"]
-HEADERS = ["icc_internal.h", "icc_device.cuh"]
+HEADERS = ["icc_internal.h", "icc_device.cuh", "icc_vec.cuh", "icc_tc.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -93,6 +93,7 @@ int cuda_fail(cudaError_t e, const char *where);
 // tensor-core mixed-precision path (icc_mixed.cu)
 void mixed_release(Op &op);
 int mixed_on_scale_update(Op &op);
+int mixed_apply_f32(Op &op, const float *x, float *y);
 int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter,
                 const icc_solve_opts &opts, double *x, int64_t *iters, double *rel_res);
 

@@ -27,6 +27,7 @@
 
 #include "icc_internal.h"
 #include "icc_device.cuh"
+#include "icc_vec.cuh"
 
 namespace icc {
 
@@ -158,60 +159,6 @@ apply_f64_kernel(Geom g, const double *__restrict__ x, const uint8_t *__restrict
     }
 }
 
-// Bricks containing node j along one direction: the brick min(j / B, nb - 1) and, for the two
-// lowest patch planes of that brick, also the previous one.  Lower brick first.
-__device__ __forceinline__ int node_bricks(int j, int B, int nb, int *bi, int *li) {
-    int i1 = min(j / B, nb - 1);
-    int l1 = j - i1 * B;
-    if (l1 <= 1 && i1 >= 1) {
-        bi[0] = i1 - 1; li[0] = l1 + B;
-        bi[1] = i1; li[1] = l1;
-        return 2;
-    }
-    bi[0] = i1; li[0] = l1;
-    return 1;
-}
-
-// y = sum of brick partials per node, output mask applied; optional partial p'y per CTA.
-__global__ void __launch_bounds__(kVecThreads)
-gather_f64_kernel(Geom g, const double *__restrict__ patch, const double *__restrict__ p,
-                  const uint8_t *__restrict__ mask, int mask_mode, double *__restrict__ y,
-                  double *__restrict__ partials, const PcgState *__restrict__ st) {
-    if (st && st->status != 0) return;
-    double dot = 0.0;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
-         n += (long long)gridDim.x * blockDim.x) {
-        int ix = int(n % g.cx), iy = int((n / g.cx) % g.cy), iz = int(n / ((long long)g.cx * g.cy));
-        int bx[2], lx[2], by[2], ly[2], bz[2], lz[2];
-        int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
-        int nby = node_bricks(iy, kBY, g.nby, by, ly);
-        int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
-        double s[3] = {0.0, 0.0, 0.0};
-        for (int a = 0; a < nbz; ++a)
-            for (int q = 0; q < nby; ++q)
-                for (int w = 0; w < nbx; ++w) {
-                    size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
-                    const double *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
-                    s[0] += pb[0];
-                    s[1] += pb[kPVol];
-                    s[2] += pb[2 * kPVol];
-                }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            long long idx = (long long)c * g.nsc + n;
-            double v = s[c];
-            if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.0;
-            else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
-            y[idx] = v;
-            if (partials) dot += p[idx] * v;
-        }
-    }
-    if (partials) {
-        dot = block_sum(dot);
-        if (threadIdx.x == 0) partials[blockIdx.x] = dot;
-    }
-}
-
 // Jacobi diagonal sum_e s_e K_type(e)[a,a]; elements visited in increasing index so the sum
 // rounds exactly as the assembled CSR entry (rust/src/sparse.rs:166-172, then :70-78).
 __global__ void __launch_bounds__(kVecThreads)
@@ -238,33 +185,7 @@ diagonal_kernel(Geom g, const double *__restrict__ scale, const int *__restrict_
     }
 }
 
-// ---- PCG vector kernels (rust/src/solver.rs:14-76) -----------------------------------------
-
-__global__ void inv_diag_kernel(long long n, const double *__restrict__ d, double *__restrict__ inv) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        inv[i] = fabs(d[i]) > 1e-12 ? 1.0 / d[i] : 1.0;
-}
-
-// x = 0, r = b, z = D^-1 r, p = z; partials: r'z and b'b
-__global__ void __launch_bounds__(kVecThreads)
-pcg_init_kernel(long long n, const double *__restrict__ b, const double *__restrict__ inv, double *__restrict__ x,
-                double *__restrict__ r, double *__restrict__ p, double *__restrict__ partials) {
-    double rz = 0.0, bb = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        double bi = b[i], zi = inv[i] * bi;
-        x[i] = 0.0;
-        r[i] = bi;
-        p[i] = zi;
-        rz += bi * zi;
-        bb += bi * bi;
-    }
-    rz = block_sum(rz);
-    bb = block_sum(bb);
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = rz;
-        partials[2 * blockIdx.x + 1] = bb;
-    }
-}
+// ---- PCG scalar steps (rust/src/solver.rs:14-76), shared by both precision forms -------------
 
 __global__ void __launch_bounds__(kVecThreads)
 pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, double tol, long long max_iter) {
@@ -287,9 +208,7 @@ pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, dou
     }
 }
 
-// p'Ap -> alpha, or breakdown (rust/src/solver.rs:41-51)
-__global__ void __launch_bounds__(kVecThreads)
-pcg_alpha_kernel(const double *__restrict__ partials, int np, PcgState *st) {
+__global__ void __launch_bounds__(kVecThreads) pcg_alpha_kernel(const double *__restrict__ partials, int np, PcgState *st) {
     if (st->status != 0) return;
     double s = 0.0;
     for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
@@ -302,32 +221,7 @@ pcg_alpha_kernel(const double *__restrict__ partials, int np, PcgState *st) {
     }
 }
 
-// x += alpha p; r -= alpha Ap; partials: r'r and r'z with z = D^-1 r (rust/src/solver.rs:52-66)
-__global__ void __launch_bounds__(kVecThreads)
-pcg_update_kernel(long long n, const double *__restrict__ p, const double *__restrict__ ap,
-                  const double *__restrict__ inv, double *__restrict__ x, double *__restrict__ r,
-                  double *__restrict__ partials, const PcgState *__restrict__ st) {
-    if (st->status != 0) return;
-    const double alpha = st->alpha;
-    double rr = 0.0, rz = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        x[i] += alpha * p[i];
-        double ri = r[i] - alpha * ap[i];
-        r[i] = ri;
-        rr += ri * ri;
-        rz += ri * (inv[i] * ri);
-    }
-    rr = block_sum(rr);
-    rz = block_sum(rz);
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = rr;
-        partials[2 * blockIdx.x + 1] = rz;
-    }
-}
-
-// relative residual test, then beta (rust/src/solver.rs:56-71)
-__global__ void __launch_bounds__(kVecThreads)
-pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st) {
+__global__ void __launch_bounds__(kVecThreads) pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st) {
     if (st->status != 0) return;
     double rr = 0.0, rz = 0.0;
     for (int i = threadIdx.x; i < np; i += blockDim.x) {
@@ -349,16 +243,6 @@ pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st) {
             if (st->iter >= st->max_iter) st->status = kStatMaxIter;
         }
     }
-}
-
-// p = D^-1 r + beta p (rust/src/solver.rs:64-71)
-__global__ void __launch_bounds__(kVecThreads)
-pcg_p_kernel(long long n, const double *__restrict__ r, const double *__restrict__ inv, double *__restrict__ p,
-             const PcgState *__restrict__ st) {
-    if (st->status != 0) return;
-    const double beta = st->beta;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        p[i] = inv[i] * r[i] + beta * p[i];
 }
 
 // ------------------------------------------------------------------------------------------
@@ -523,7 +407,7 @@ void Op::enqueue_apply(const double *x, double *y, double *partials, const PcgSt
     apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
         g, x, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
         st);
-    gather_f64_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, x, d_mask, mask_mode, y, partials, st);
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, x, d_mask, mask_mode, y, partials, st);
 }
 
 int Op::apply_dev(const double *x, double *y) {
@@ -556,9 +440,9 @@ int Op::ensure_pcg_buffers() {
 void Op::enqueue_pcg_iteration() {
     enqueue_apply(d_p, d_ap, d_partials, d_state);
     pcg_alpha_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
-    pcg_update_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials, d_state);
+    pcg_update_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials, d_state);
     pcg_beta_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
-    pcg_p_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_r, d_inv, d_p, d_state);
+    pcg_p_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_r, d_inv, d_p, d_state);
 }
 
 int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_iter, int check_every, double *x,
@@ -571,8 +455,8 @@ int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_it
         diag = d_diag;
         launches += 1;
     }
-    inv_diag_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, diag, d_inv);
-    pcg_init_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(ndof, b, d_inv, d_x, d_r, d_p, d_partials);
+    inv_diag_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, diag, d_inv);
+    pcg_init_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, b, d_inv, d_x, d_r, d_p, d_partials);
     pcg_init_finalize<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state, tol, max_iter);
     ICC_CUDA(cudaGetLastError(), "pcg init");
     if (check_every <= 0) check_every = 32;
@@ -697,6 +581,27 @@ int icc_op_apply(icc_op *op, const double *x, double *y, int64_t n) {
     return ICC_OK;
 }
 
+int icc_op_apply_f32_dev(icc_op *op, const float *x, float *y, int64_t n) {
+    if (!op || !x || !y) return set_error(ICC_BAD_ARG, "icc_op_apply_f32_dev: null argument");
+    if (n != op->op.ndof) return set_error(ICC_BAD_ARG, "icc_op_apply_f32_dev: n != ndof");
+    cudaSetDevice(op->op.device);
+    return icc::mixed_apply_f32(op->op, x, y);
+}
+
+int icc_op_apply_f32(icc_op *op, const float *x, float *y, int64_t n) {
+    if (!op || !x || !y) return set_error(ICC_BAD_ARG, "icc_op_apply_f32: null argument");
+    icc::Op &o = op->op;
+    if (n != o.ndof) return set_error(ICC_BAD_ARG, "icc_op_apply_f32: n != ndof");
+    cudaSetDevice(o.device);
+    float *xd = reinterpret_cast<float *>(o.d_x_in), *yd = reinterpret_cast<float *>(o.d_y_out);
+    ICC_CUDA(cudaMemcpyAsync(xd, x, (size_t)n * 4, cudaMemcpyHostToDevice, o.stream), "apply_f32 h2d");
+    int rc = icc::mixed_apply_f32(o, xd, yd);
+    if (rc) return rc;
+    ICC_CUDA(cudaMemcpyAsync(y, yd, (size_t)n * 4, cudaMemcpyDeviceToHost, o.stream), "apply_f32 d2h");
+    ICC_CUDA(cudaStreamSynchronize(o.stream), "apply_f32 sync");
+    return ICC_OK;
+}
+
 int icc_op_diagonal(icc_op *op, double *d, int64_t n) {
     if (!op || !d) return set_error(ICC_BAD_ARG, "icc_op_diagonal: null argument");
     icc::Op &o = op->op;
@@ -777,7 +682,7 @@ int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t
             o.g, x_dev, o.d_mask, o.mask_mode != ICC_MASK_NONE, o.d_scale, o.d_kfrag, o.d_tile_start, o.d_tile_type,
             o.d_tile_elem, o.d_patch, nullptr);
         cudaEventRecord(ev[3 * r + 1], o.stream);
-        icc::gather_f64_kernel<<<o.vec_blocks, icc::kVecThreads, 0, o.stream>>>(o.g, o.d_patch, x_dev, o.d_mask,
+        icc::gather_kernel<double><<<o.vec_blocks, icc::kVecThreads, 0, o.stream>>>(o.g, o.d_patch, x_dev, o.d_mask,
                                                                                 o.mask_mode, y_dev, nullptr, nullptr);
         cudaEventRecord(ev[3 * r + 2], o.stream);
     }

@@ -1,0 +1,144 @@
+// Node-side sum of brick partials and the PCG vector kernels, templated on the vector type:
+// T = double for the FP64 solve, T = float for the inner solve of the mixed form.  Every
+// reduction accumulates in double with a fixed-shape two-stage tree (per-CTA partials, then one
+// CTA), so results are reproducible run to run.
+#pragma once
+
+#include "icc_device.cuh"
+
+namespace icc {
+
+// Bricks containing node j along one direction: the brick min(j / B, nb - 1) and, for the two
+// lowest patch planes of that brick, also the previous one.  Lower brick first.
+__device__ __forceinline__ int node_bricks(int j, int B, int nb, int *bi, int *li) {
+    int i1 = min(j / B, nb - 1);
+    int l1 = j - i1 * B;
+    if (l1 <= 1 && i1 >= 1) {
+        bi[0] = i1 - 1;
+        li[0] = l1 + B;
+        bi[1] = i1;
+        li[1] = l1;
+        return 2;
+    }
+    bi[0] = i1;
+    li[0] = l1;
+    return 1;
+}
+
+// y = sum of the brick partials of each node (fixed order), output mask applied;
+// optionally the CTA partial of p'y (in double).
+template <class T>
+__global__ void __launch_bounds__(kVecThreads)
+gather_kernel(Geom g, const T *__restrict__ patch, const T *__restrict__ p, const uint8_t *__restrict__ mask,
+              int mask_mode, T *__restrict__ y, double *__restrict__ partials, const PcgState *__restrict__ st) {
+    if (st && st->status != 0) return;
+    double dot = 0.0;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
+         n += (long long)gridDim.x * blockDim.x) {
+        int ix = int(n % g.cx), iy = int((n / g.cx) % g.cy), iz = int(n / ((long long)g.cx * g.cy));
+        int bx[2], lx[2], by[2], ly[2], bz[2], lz[2];
+        int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
+        int nby = node_bricks(iy, kBY, g.nby, by, ly);
+        int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
+        T s0 = T(0), s1 = T(0), s2 = T(0);
+        for (int a = 0; a < nbz; ++a)
+            for (int q = 0; q < nby; ++q)
+                for (int w = 0; w < nbx; ++w) {
+                    size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
+                    const T *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
+                    s0 += pb[0];
+                    s1 += pb[kPVol];
+                    s2 += pb[2 * kPVol];
+                }
+        T sv[3] = {s0, s1, s2};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            long long idx = (long long)c * g.nsc + n;
+            T v = sv[c];
+            if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = T(0);
+            else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
+            y[idx] = v;
+            if (partials) dot += double(p[idx]) * double(v);
+        }
+    }
+    if (partials) {
+        dot = block_sum(dot);
+        if (threadIdx.x == 0) partials[blockIdx.x] = dot;
+    }
+}
+
+// ---- PCG vector kernels (rust/src/solver.rs:14-76) -----------------------------------------
+
+template <class T>
+__global__ void inv_diag_kernel(long long n, const double *__restrict__ d, T *__restrict__ inv) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        inv[i] = T(fabs(d[i]) > 1e-12 ? 1.0 / d[i] : 1.0);
+}
+
+// x = 0, r = b, z = D^-1 r, p = z; partials: r'z and b'b   (rust/src/solver.rs:15-36)
+template <class T>
+__global__ void __launch_bounds__(kVecThreads)
+pcg_init_kernel(long long n, const T *__restrict__ b, const T *__restrict__ inv, T *__restrict__ x,
+                T *__restrict__ r, T *__restrict__ p, double *__restrict__ partials) {
+    double rz = 0.0, bb = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        T bi = b[i], zi = inv[i] * bi;
+        x[i] = T(0);
+        r[i] = bi;
+        p[i] = zi;
+        rz += double(bi) * double(zi);
+        bb += double(bi) * double(bi);
+    }
+    rz = block_sum(rz);
+    bb = block_sum(bb);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = rz;
+        partials[2 * blockIdx.x + 1] = bb;
+    }
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, double tol, long long max_iter);
+
+// p'Ap -> alpha, or breakdown (rust/src/solver.rs:41-51)
+__global__ void __launch_bounds__(kVecThreads) pcg_alpha_kernel(const double *__restrict__ partials, int np, PcgState *st);
+
+// relative residual test, then beta (rust/src/solver.rs:56-71)
+__global__ void __launch_bounds__(kVecThreads) pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st);
+
+// x += alpha p; r -= alpha Ap; partials: r'r and r'z with z = D^-1 r (rust/src/solver.rs:52-66)
+template <class T>
+__global__ void __launch_bounds__(kVecThreads)
+pcg_update_kernel(long long n, const T *__restrict__ p, const T *__restrict__ ap, const T *__restrict__ inv,
+                  T *__restrict__ x, T *__restrict__ r, double *__restrict__ partials,
+                  const PcgState *__restrict__ st) {
+    if (st->status != 0) return;
+    const T alpha = T(st->alpha);
+    double rr = 0.0, rz = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        T ri = r[i] - alpha * ap[i];
+        r[i] = ri;
+        rr += double(ri) * double(ri);
+        rz += double(ri) * double(inv[i] * ri);
+    }
+    rr = block_sum(rr);
+    rz = block_sum(rz);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = rr;
+        partials[2 * blockIdx.x + 1] = rz;
+    }
+}
+
+// p = D^-1 r + beta p (rust/src/solver.rs:64-71)
+template <class T>
+__global__ void __launch_bounds__(kVecThreads)
+pcg_p_kernel(long long n, const T *__restrict__ r, const T *__restrict__ inv, T *__restrict__ p,
+             const PcgState *__restrict__ st) {
+    if (st->status != 0) return;
+    const T beta = T(st->beta);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = inv[i] * r[i] + beta * p[i];
+}
+
+}  // namespace icc

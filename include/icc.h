@@ -107,6 +107,10 @@ int icc_op_update_mask(icc_op *op, const uint8_t *free_mask, int32_t mask_mode);
 int icc_op_apply(icc_op *op, const double *x, double *y, int64_t n);
 /* Same on device arrays, enqueued on the handle's stream (see icc_op_stream). */
 int icc_op_apply_dev(icc_op *op, const double *x_dev, double *y_dev, int64_t n);
+/* y = A x in FP32 with the tensor-core contraction (3-term split-TF32 products, FP32
+ * accumulation): the operator of the ICC_MIXED inner solve.  Host arrays / device arrays. */
+int icc_op_apply_f32(icc_op *op, const float *x, float *y, int64_t n);
+int icc_op_apply_f32_dev(icc_op *op, const float *x_dev, float *y_dev, int64_t n);
 /* CsrMatrix::diagonal (rust/src/sparse.rs:70-78) of the unmasked operator: sum_e s_e K[a,a],
  * accumulated in element order, bit-identical to the assembled CSR diagonal. */
 int icc_op_diagonal(icc_op *op, double *d, int64_t n);
