@@ -43,6 +43,7 @@ EXPORTED = [
     "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_apply_f32",
     "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
+    "icc_apply_f64_noalloc",
 ]
 
 
@@ -106,6 +107,7 @@ def lib():
                                     C.POINTER(i64), C.POINTER(dbl)]
     L.icc_op_last_solve_info.argtypes = [vp, C.POINTER(SolveInfo)]
     L.icc_op_profile_apply.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
+    L.icc_apply_f64_noalloc.argtypes = [i64p, vp, i32, vp, vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -287,3 +289,11 @@ class PcgSolver:
                                      C.byref(it), C.byref(res))
         self.status = _check(rc, (ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN))
         return it.value, res.value
+
+
+def apply_f64_noalloc(nel_dir, ke_ptr, ntypes, type_id_ptr, scale_ptr, x_ptr, y_ptr, stream=0):
+    """icc_apply_f64_noalloc on caller-owned device buffers (raw pointers); allocates nothing."""
+    ne = np.ascontiguousarray(np.asarray(nel_dir, dtype=np.int64))
+    _check(lib().icc_apply_f64_noalloc(ne, C.c_void_p(ke_ptr), int(ntypes), C.c_void_p(type_id_ptr),
+                                       C.c_void_p(scale_ptr) if scale_ptr else None, C.c_void_p(x_ptr),
+                                       C.c_void_p(y_ptr), C.c_void_p(stream) if stream else None))

@@ -131,6 +131,21 @@ int icc_pcg_solve_dev(icc_op *op, const double *b_dev, const double *diag_dev, i
 /* Details of the last solve on this handle. */
 int icc_op_last_solve_info(const icc_op *op, icc_solve_info *info);
 
+/* ---- allocation-free apply (no counterpart in the reference) --------------------------------
+ * y = K x (FP64, no mask) for callers that must not allocate device memory: applications that
+ * hand libraries buffers from their own device pool and forbid cudaMalloc/cudaFree (which can
+ * synchronize the device), or loops that may not allocate after start-up.  Every argument is a
+ * buffer the caller owns: nel_dir (host), ke_types_dev [ntypes*81*81] row-major, type_id_dev [nel],
+ * scale_dev [nel] or NULL for 1, x_dev / y_dev [ndof]; stream is a cudaStream_t (NULL = default).
+ * The only scratch is a fixed 16 MiB device array inside the library (held on every GPU that loads
+ * it until exit), so grids are limited to 1941 bricks of 8x4x4 elements (for example 96x48x48
+ * elements); larger grids return ICC_BAD_ARG.  The first call on a device resolves that array's
+ * address (make it before any stream capture).  All calls share the array: calls that overlap on
+ * the GPU race and must be ordered by the caller.  Allocates nothing. */
+int icc_apply_f64_noalloc(const int64_t nel_dir[3], const double *ke_types_dev, int32_t ntypes,
+                          const int32_t *type_id_dev, const double *scale_dev, const double *x_dev, double *y_dev,
+                          void *stream);
+
 /* ---- diagnostics (no reference counterpart) -------------------------------------------------
  * Times `reps` FP64 applies of x_dev on the handle's stream with CUDA events around each of the
  * two kernels of an apply (the element-brick contraction and the node-side sum); returns the
