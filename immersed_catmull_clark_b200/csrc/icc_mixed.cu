@@ -16,6 +16,7 @@
 // vectors are FP32 with FP64 dot products.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -36,18 +37,9 @@ constexpr int kTcM = kEPB;        // 128 rows = the brick's elements
 constexpr int kTcN = 96;          // test DOFs 81 -> 96
 constexpr int kTcK = 88;          // trial DOFs 81 -> 88 = 11 MMAs of K = 8
 constexpr int kTcKSteps = kTcK / 8;
-constexpr int kAFl = kTcM * kTcK;  // floats per A term
 constexpr int kBFl = kTcN * kTcK;  // floats per B term
-constexpr uint32_t kALbo = (kTcM / 8) * 128;  // bytes between K-adjacent core matrices of A
-constexpr uint32_t kBLbo = (kTcN / 8) * 128;
+constexpr uint32_t kBLbo = (kTcN / 8) * 128;  // bytes between K-adjacent core matrices of B
 constexpr uint32_t kSbo = 128;                // bytes between 8-row groups
-constexpr int kTcThreads = 128;
-constexpr int kTcSmemUsed = (2 * kAFl + 2 * kBFl + 3 * kPVol) * 4;
-// allocation rounded up to 176 KB: the operand descriptors can never address past the CTA's
-// shared memory, even if an 8-row-group stride and a K-chunk stride were interchanged
-constexpr int kTcSmem = 176 * 1024;
-static_assert(kTcSmemUsed <= kTcSmem, "shared memory budget");
-constexpr uint32_t kTmemCols = 256;  // D uses 96; one CTA per SM
 constexpr long long kWaitLimit = 1LL << 22;
 
 // offset (floats) of element (row, k) in the canonical K-major no-swizzle layout with `rows` rows
@@ -65,6 +57,7 @@ struct MixedState {
           *d_inv32 = nullptr;
     double *d_x64 = nullptr, *d_r64 = nullptr, *d_y64 = nullptr, *d_scalars = nullptr;
     int *d_err = nullptr;
+    int main_type = 0;               // most frequent pass type: pinned in B buffer 0
     PcgState *d_state = nullptr, *h_state = nullptr;
     double *h_scalars = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -75,161 +68,273 @@ struct MixedState {
 // Kernels
 // ------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kTcThreads, 1)
+// ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
+// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles:
+//   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; split the current
+//     brick's gathered element vectors into TF32 hi/lo and store them as the A operand straight
+//     into TMEM (row m = element m = lane m), double-buffered in two A slots;
+//   warp 8 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
+//     element type, buffer 1 for the others, fetched with cp.async.bulk), issues the 33
+//     tcgen05.mma (A from TMEM, B from shared memory) per type pass into one TMEM accumulator;
+//   warps 4-7 (epilogue): drain the accumulator with tcgen05.ld, keep each row's own type pass,
+//     scale by s_e, stage the rows in shared memory and write the brick's patch partial sums.
+// mbarriers: a_full[2] (builders -> MMA), a_empty[2] (MMA commit -> builders), d_full (MMA commit
+// -> epilogue), d_empty (epilogue -> MMA), b_full[2] (bulk copies).  Every wait is bounded; on
+// time-out the CTA raises a shared abort flag, so all roles finish promptly and the host reports
+// ICC_TIMEOUT.
+constexpr int kPtThreads = 288;
+constexpr int kColSlot = 176;    // A slot s: hi at s*176 + [0,88), lo at s*176 + 88 + [0,88)
+constexpr int kColD = 352;       // accumulator: 96 columns
+constexpr uint32_t kPtTmemCols = 512;
+constexpr int kPtSmem = (4 * kBFl + 2 * 3 * kPVol + kEPB * 81) * 4;  // 185,280 B
+constexpr uint32_t kBBytes = 2 * kBFl * 4;                            // one type, hi + lo
+
+__device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        if (tc::mbar_try_wait(bar, parity)) return true;
+        if (*abort_flag) return false;
+    }
+    *abort_flag = 1;
+    atomicExch(err, 1);
+    return false;
+}
+
+struct BrickBox {
+    int x0, y0, z0, ex_n, ey_n, ez_n;
+};
+
+__device__ __forceinline__ BrickBox brick_box(const Geom &g, int b) {
+    BrickBox r;
+    const int bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / (g.nbx * g.nby);
+    r.x0 = bxi * kBX;
+    r.y0 = byi * kBY;
+    r.z0 = bzi * kBZ;
+    r.ex_n = min(kBX, g.nx - r.x0);
+    r.ey_n = min(kBY, g.ny - r.y0);
+    r.ez_n = min(kBZ, g.nz - r.z0);
+    return r;
+}
+
+__global__ void __launch_bounds__(kPtThreads, 1)
 apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__ mask, int mask_in,
                 const float *__restrict__ scale, const int *__restrict__ type_id, const float4 *__restrict__ bmat,
-                const int *__restrict__ pass_start, const int *__restrict__ pass_type, float *__restrict__ patch_out,
-                int *__restrict__ err, const PcgState *__restrict__ st) {
+                int main_type, const int *__restrict__ pass_start, const int *__restrict__ pass_type,
+                float *__restrict__ patch_out, int *__restrict__ err, const PcgState *__restrict__ st) {
     if (st && st->status != 0) return;
-    extern __shared__ __align__(1024) float tsm[];
-    float *sA = tsm;                 // [2][kAFl]  A_hi, A_lo; reused as Y[128][81] after the MMAs
-    float *sB = tsm + 2 * kAFl;      // [2][kBFl]  B_hi, B_lo
-    float *sP = sB + 2 * kBFl;       // [3][kPVol] input patch
-    __shared__ __align__(8) uint64_t mbar;
+    extern __shared__ __align__(1024) float psm[];
+    float *sB = psm;                      // [2 buffers][hi, lo][kBFl]
+    float *sP = psm + 4 * kBFl;           // [2][3 * kPVol]
+    float *sY = sP + 2 * 3 * kPVol;       // [kEPB][81]
+    __shared__ __align__(8) uint64_t bars[8];
     __shared__ uint32_t tmem_base;
+    __shared__ int s_koff[88];
+    __shared__ volatile int s_abort;
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *b_full = bars + 6;
 
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int b = blockIdx.x;
-    const int bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / (g.nbx * g.nby);
-    const int x0 = bxi * kBX, y0 = byi * kBY, z0 = bzi * kBZ;
-    const int ex_n = min(kBX, g.nx - x0), ey_n = min(kBY, g.ny - y0), ez_n = min(kBZ, g.nz - z0);
-
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, kTmemCols);
+        tc::tmem_alloc(&tmem_base, kPtTmemCols);
         tc::tmem_relinquish();
     }
-    if (tid == 0) {
-        tc::mbar_init(&mbar, 1);
-        tc::fence_mbar_init();
+    if (tid < 88) {
+        int k = tid;
+        int c = k / 27, a = k % 27;
+        s_koff[tid] = k < 81 ? c * kPVol + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3 : -1;
     }
-    for (int i = tid; i < 3 * kPVol; i += kTcThreads) {
-        int c = i / kPVol, r = i - c * kPVol;
-        int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
-        int gx = x0 + px, gy = y0 + py, gz = z0 + pz;
-        float v = 0.f;
-        if (gx < g.cx && gy < g.cy && gz < g.cz) {
-            long long idx = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + gx;
-            v = x[idx];
-            if (mask_in && !mask[idx]) v = 0.f;
-        }
-        sP[i] = v;
+    if (tid == 0) {
+        tc::mbar_init(&a_full[0], 128);
+        tc::mbar_init(&a_full[1], 128);
+        tc::mbar_init(&a_empty[0], 1);
+        tc::mbar_init(&a_empty[1], 1);
+        tc::mbar_init(d_full, 1);
+        tc::mbar_init(d_empty, 128);
+        tc::mbar_init(&b_full[0], 1);
+        tc::mbar_init(&b_full[1], 1);
+        tc::fence_mbar_init();
+        s_abort = 0;
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
+    const int nmine = blockIdx.x < g.nbricks ? (g.nbricks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
-    // this thread's element (row m of the tile)
-    const int m = tid;
-    const int lx = m % kBX, ly = (m / kBX) % kBY, lz = m / (kBX * kBY);
-    const bool valid = lx < ex_n && ly < ey_n && lz < ez_n;
-    int my_type = -1;
-    float s = 0.f;
-    if (valid) {
-        long long eg = (long long)(x0 + lx) + (long long)g.nx * ((y0 + ly) + (long long)g.ny * (z0 + lz));
-        my_type = type_id[eg];
-        s = scale[eg];
-    }
-    const int base = (lz * kPY + ly) * kPX + lx;
-    // A rows: split each value into hi + lo TF32 parts, 16-byte stores along K
-#pragma unroll 1
-    for (int ch = 0; ch < kTcK / 4; ++ch) {
-        float hi[4], lo[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int k = ch * 4 + q;
-            float v = 0.f;
-            if (valid && k < 81) {
-                int c = k / 27, a = k % 27;
-                v = sP[c * kPVol + base + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
+    if (warp < 4) {
+        // ------------------------------ builders ------------------------------
+        const int m = tid;
+        const int lx = m % kBX, ly = (m / kBX) % kBY, lz = m / (kBX * kBY);
+        const int base = (lz * kPY + ly) * kPX + lx;
+        auto load_patch = [&](int b, float *dst) {
+            BrickBox bb = brick_box(g, b);
+            for (int i = m; i < 3 * kPVol; i += 128) {
+                int c = i / kPVol, r = i - c * kPVol;
+                int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
+                int gx = bb.x0 + px, gy = bb.y0 + py, gz = bb.z0 + pz;
+                if (gx < g.cx && gy < g.cy && gz < g.cz)
+                    tc::cp_async4(dst + i, x + ((long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + gx));
+                else
+                    dst[i] = 0.f;
             }
-            hi[q] = tc::to_tf32(v);
-            lo[q] = tc::to_tf32(v - hi[q]);
-        }
-        int off = canon(m, ch * 4, kTcM);
-        *reinterpret_cast<float4 *>(sA + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<float4 *>(sA + kAFl + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-    }
-    tc::fence_proxy_async();
-
-    float res[81];
-#pragma unroll
-    for (int n = 0; n < 81; ++n) res[n] = 0.f;
-    constexpr uint32_t idesc = tc::idesc_tf32(kTcM, kTcN);
-    const int p0 = pass_start[b], p1 = pass_start[b + 1];
-    bool timed_out = false;
-    for (int pi = p0; pi < p1; ++pi) {
-        const int t = pass_type[pi];
-        const float4 *src = bmat + (size_t)t * (2 * kBFl / 4);
-        float4 *dst = reinterpret_cast<float4 *>(sB);
-        for (int i = tid; i < 2 * kBFl / 4; i += kTcThreads) dst[i] = src[i];
-        tc::fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
+            tc::cp_async_commit();
+        };
+        if (nmine > 0) load_patch(blockIdx.x, sP);
+        for (int it = 0; it < nmine; ++it) {
+            const int b = blockIdx.x + it * gridDim.x;
+            const int s = it & 1;
+            float *P = sP + s * 3 * kPVol;
+            if (it + 1 < nmine) load_patch(b + gridDim.x, sP + ((it + 1) & 1) * 3 * kPVol);
+            else tc::cp_async_commit();
+            tc::cp_async_wait<1>();
+            const BrickBox bb = brick_box(g, b);
+            if (mask_in) {
+                for (int i = m; i < 3 * kPVol; i += 128) {
+                    int c = i / kPVol, r = i - c * kPVol;
+                    int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
+                    int gx = bb.x0 + px, gy = bb.y0 + py, gz = bb.z0 + pz;
+                    if (gx < g.cx && gy < g.cy && gz < g.cz &&
+                        !mask[(long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + gx])
+                        P[i] = 0.f;
+                }
+            }
+            tc::named_sync(1, 128);
+            if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
+            const bool valid = lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n;
+            const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kColSlot);
 #pragma unroll 1
-            for (int ks = 0; ks < kTcKSteps; ++ks) {
-                const float *a_hi = sA + ks * 2 * (kTcM / 8) * 32;
-                const float *b_hi = sB + ks * 2 * (kTcN / 8) * 32;
-                uint64_t ah = tc::make_desc(a_hi, kALbo, kSbo), al = tc::make_desc(a_hi + kAFl, kALbo, kSbo);
-                uint64_t bh = tc::make_desc(b_hi, kBLbo, kSbo), bl = tc::make_desc(b_hi + kBFl, kBLbo, kSbo);
-                tc::mma_tf32(tmem, al, bh, idesc, ks > 0 ? 1u : 0u);
-                tc::mma_tf32(tmem, ah, bl, idesc, 1u);
-                tc::mma_tf32(tmem, ah, bh, idesc, 1u);
+            for (int c8 = 0; c8 < kTcK / 8; ++c8) {
+                float hi[8], lo[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int off = s_koff[c8 * 8 + q];
+                    const float v = (valid && off >= 0) ? P[off + base] : 0.f;
+                    hi[q] = tc::to_tf32(v);
+                    lo[q] = tc::to_tf32(v - hi[q]);
+                }
+                tc::tmem_st8(trow + c8 * 8, hi);
+                tc::tmem_st8(trow + kTcK + c8 * 8, lo);
             }
-            tc::mma_commit(&mbar);
+            tc::tmem_wait_st();
+            tc::fence_before_sync();
+            tc::mbar_arrive(&a_full[s]);
+            tc::named_sync(1, 128);   // everyone is done with P before the next prefetch reuses it
         }
-        const bool ok = tc::mbar_wait_bounded(&mbar, uint32_t(pi - p0) & 1u, kWaitLimit);
-        timed_out = __syncthreads_or(!ok) != 0;  // CTA-uniform decision
-        if (timed_out) {
-            if (tid == 0) atomicExch(err, 1);
-            tc::mbar_wait_bounded(&mbar, uint32_t(pi - p0) & 1u, kWaitLimit);  // let issued MMAs drain
-        }
-        tc::fence_after_sync();
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-        for (int cc = 0; cc < kTcN / 16; ++cc) {
-            uint32_t r[16];
-            tc::tmem_ld16(taddr + cc * 16, r);
-            tc::tmem_wait_ld();
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int n = cc * 16 + j;
-                if (n < 81 && my_type == t) res[n] = s * __uint_as_float(r[j]);
+        tc::cp_async_wait<0>();
+    } else if (warp < 8) {
+        // ------------------------------ epilogue ------------------------------
+        const int q4 = warp & 3;
+        const int r = q4 * 32 + lane;   // TMEM lane quadrant of this warp = its rows
+        const int et = tid - 128;       // 0..127 for the node sum
+        const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
+        const uint32_t dcol = tmem + ((uint32_t)(q4 * 32) << 16) + kColD;
+        int j = 0;
+        for (int it = 0; it < nmine; ++it) {
+            const int b = blockIdx.x + it * gridDim.x;
+            const BrickBox bb = brick_box(g, b);
+            const bool valid = lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n;
+            int my_type = -1;
+            float se = 0.f;
+            if (valid) {
+                long long eg = (long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz));
+                my_type = type_id[eg];
+                se = scale[eg];
             }
-        }
-        tc::fence_before_sync();
-        __syncthreads();
-        if (timed_out) break;
-    }
-
-    // stage the scaled element results (A is no longer read by the tensor core)
-    float *sY = sA;
-    if (valid) {
+            const int p0 = pass_start[b], p1 = pass_start[b + 1];
+            float res[81];
 #pragma unroll
-        for (int n = 0; n < 81; ++n) sY[m * 81 + n] = res[n];
-    }
-    __syncthreads();
-    float *outb = patch_out + (size_t)b * 3 * kPVol;
-    for (int i = tid; i < 3 * kPVol; i += kTcThreads) {
-        int c = i / kPVol, r = i - c * kPVol;
-        int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
-        float sum = 0.f;
-        if (px < ex_n + 2 && py < ey_n + 2 && pz < ez_n + 2) {
-            for (int qz = max(pz - 2, 0); qz <= min(pz, ez_n - 1); ++qz)
-                for (int qy = max(py - 2, 0); qy <= min(py, ey_n - 1); ++qy)
-                    for (int qx = max(px - 2, 0); qx <= min(px, ex_n - 1); ++qx) {
-                        int e = qx + kBX * (qy + kBY * qz);
-                        sum += sY[e * 81 + c * 27 + (px - qx) + 3 * (py - qy) + 9 * (pz - qz)];
+            for (int n = 0; n < 81; ++n) res[n] = 0.f;
+            for (int pi = p0; pi < p1; ++pi, ++j) {
+                const int t = pass_type[pi];
+                pt_wait(d_full, uint32_t(j) & 1u, &s_abort, err);
+                tc::fence_after_sync();
+#pragma unroll
+                for (int cc = 0; cc < kTcN / 16; ++cc) {
+                    uint32_t rr[16];
+                    tc::tmem_ld16(dcol + cc * 16, rr);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        const int n = cc * 16 + q;
+                        if (n < 81 && my_type == t) res[n] = se * __uint_as_float(rr[q]);
                     }
+                }
+                tc::fence_before_sync();
+                tc::mbar_arrive(d_empty);
+            }
+            tc::named_sync(2, 128);   // the previous brick's node sum is done with sY
+            if (valid) {
+#pragma unroll
+                for (int n = 0; n < 81; ++n) sY[r * 81 + n] = res[n];
+            }
+            tc::named_sync(2, 128);
+            float *outb = patch_out + (size_t)b * 3 * kPVol;
+            for (int i = et; i < 3 * kPVol; i += 128) {
+                int c = i / kPVol, rem = i - c * kPVol;
+                int px = rem % kPX, py = (rem / kPX) % kPY, pz = rem / (kPX * kPY);
+                float sum = 0.f;
+                if (px < bb.ex_n + 2 && py < bb.ey_n + 2 && pz < bb.ez_n + 2) {
+                    for (int qz = max(pz - 2, 0); qz <= min(pz, bb.ez_n - 1); ++qz)
+                        for (int qy = max(py - 2, 0); qy <= min(py, bb.ey_n - 1); ++qy)
+                            for (int qx = max(px - 2, 0); qx <= min(px, bb.ex_n - 1); ++qx) {
+                                int e = qx + kBX * (qy + kBY * qz);
+                                sum += sY[e * 81 + c * 27 + (px - qx) + 3 * (py - qy) + 9 * (pz - qz)];
+                            }
+                }
+                outb[i] = sum;
+            }
         }
-        outb[i] = sum;
+    } else if (lane == 0) {
+        // ------------------------------ MMA issuer ------------------------------
+        constexpr uint32_t idesc = tc::idesc_tf32(kTcM, kTcN);
+        tc::mbar_arrive_expect_tx(&b_full[0], kBBytes);
+        tc::bulk_g2s(sB, bmat + (size_t)main_type * (2 * kBFl / 4), kBBytes, &b_full[0]);
+        pt_wait(&b_full[0], 0u, &s_abort, err);
+        int tag1 = -1;
+        uint32_t b1_phase = 0;
+        int j = 0;
+        for (int it = 0; it < nmine; ++it) {
+            const int b = blockIdx.x + it * gridDim.x;
+            const int s = it & 1;
+            pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
+            const int p0 = pass_start[b], p1 = pass_start[b + 1];
+            for (int pi = p0; pi < p1; ++pi, ++j) {
+                const int t = pass_type[pi];
+                // the previous pass has been drained: no MMA still reads D or a B buffer
+                if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
+                int buf = 0;
+                if (t != main_type) {
+                    buf = 1;
+                    if (tag1 != t) {
+                        tc::mbar_arrive_expect_tx(&b_full[1], kBBytes);
+                        tc::bulk_g2s(sB + 2 * kBFl, bmat + (size_t)t * (2 * kBFl / 4), kBBytes, &b_full[1]);
+                        pt_wait(&b_full[1], b1_phase & 1u, &s_abort, err);
+                        b1_phase++;
+                        tag1 = t;
+                    }
+                }
+                tc::fence_after_sync();
+                const float *bh0 = sB + buf * 2 * kBFl;
+                const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
+#pragma unroll 1
+                for (int ks = 0; ks < kTcKSteps; ++ks) {
+                    const float *bh = bh0 + ks * 2 * (kTcN / 8) * 32;
+                    const uint64_t dbh = tc::make_desc(bh, kBLbo, kSbo), dbl = tc::make_desc(bh + kBFl, kBLbo, kSbo);
+                    const uint32_t ah = acol + ks * 8, al = acol + kTcK + ks * 8;
+                    tc::mma_tf32_ts(tmem + kColD, al, dbh, idesc, ks > 0 ? 1u : 0u);
+                    tc::mma_tf32_ts(tmem + kColD, ah, dbl, idesc, 1u);
+                    tc::mma_tf32_ts(tmem + kColD, ah, dbh, idesc, 1u);
+                }
+                tc::mma_commit(d_full);
+            }
+            tc::mma_commit(&a_empty[s]);
+        }
+        if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
     }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, kTmemCols);
+        tc::tmem_dealloc(tmem, kPtTmemCols);
     }
 }
 
@@ -355,6 +460,14 @@ static int mixed_init(Op &op) {
         for (int t : seen) ptype.push_back(t);
         pstart.push_back(int(ptype.size()));
     }
+    {
+        std::vector<int> count((size_t)op.ntypes, 0);
+        for (int t : ptype) count[(size_t)t]++;
+        int best = 0;
+        for (int t = 1; t < op.ntypes; ++t)
+            if (count[(size_t)t] > count[(size_t)best]) best = t;
+        ms.main_type = best;
+    }
     if ((rc = dalloc(&ms.d_pass_start, pstart.size(), "alloc passes"))) return rc;
     if ((rc = dalloc(&ms.d_pass_type, ptype.size(), "alloc passes"))) return rc;
     ICC_CUDA(cudaMemcpy(ms.d_pass_start, pstart.data(), pstart.size() * 4, cudaMemcpyHostToDevice), "copy passes");
@@ -374,7 +487,7 @@ static int mixed_init(Op &op) {
     ICC_CUDA(cudaMallocHost((void **)&ms.h_state, sizeof(PcgState)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&ms.h_scalars, 8 * sizeof(double)), "alloc pinned");
     ICC_CUDA(cudaMemset(ms.d_err, 0, sizeof(int)), "clear err");
-    ICC_CUDA(cudaFuncSetAttribute(apply_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem),
+    ICC_CUDA(cudaFuncSetAttribute(apply_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPtSmem),
              "cudaFuncSetAttribute tc");
     ms.ready = true;
     return mixed_on_scale_update(op);
@@ -404,27 +517,33 @@ int mixed_on_scale_update(Op &op) {
 }
 
 // enqueue y32 = A p32 with the tensor-core apply (partials: p'Ap per CTA)
-static void enqueue_apply_tc(Op &op, const float *x, float *y, double *partials, const PcgState *st) {
+static void enqueue_apply_tc(Op &op, const float *x, float *y, double *partials, const PcgState *st,
+                             bool input_masked = false) {
     MixedState &ms = *op.mixed;
-    apply_tc_kernel<<<op.g.nbricks, kTcThreads, kTcSmem, op.stream>>>(
-        op.g, x, op.d_mask, op.mask_mode != ICC_MASK_NONE, ms.d_scale32, op.d_type_id, ms.d_bmat, ms.d_pass_start,
-        ms.d_pass_type, ms.d_patch32, ms.d_err, st);
+    const int grid = std::min(op.num_sms, op.g.nbricks);
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(
+        op.g, x, op.d_mask, (op.mask_mode != ICC_MASK_NONE && !input_masked) ? 1 : 0, ms.d_scale32, op.d_type_id,
+        ms.d_bmat, ms.main_type, ms.d_pass_start, ms.d_pass_type, ms.d_patch32, ms.d_err, st);
     gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, x, op.d_mask, op.mask_mode,
                                                                        y, partials, st);
 }
 
+// One iteration of the FP32 (sloppy) PCG on the tensor-core operator.  With ICC_MASK_ZERO the
+// search direction is kept zero on fixed DOFs, so the apply needs no input mask.
 static void enqueue_inner_iteration(Op &op) {
     MixedState &ms = *op.mixed;
     const int vb = op.vec_blocks;
-    enqueue_apply_tc(op, ms.d_p32, ms.d_ap32, op.d_partials, ms.d_state);
+    const bool pre = op.mask_mode == ICC_MASK_ZERO;
+    const uint8_t *pm = pre ? op.d_mask : nullptr;
+    enqueue_apply_tc(op, ms.d_p32, ms.d_ap32, op.d_partials, ms.d_state, pre);
     pcg_alpha_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
     pcg_update_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_p32, ms.d_ap32, ms.d_inv32, ms.d_x32,
                                                                 ms.d_r32, op.d_partials, ms.d_state);
     pcg_beta_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
-    pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state);
+    pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state, pm);
 }
 
-// Diagnostic / test hook: y32 = A x32 on the tensor cores (used by the mixed apply test path).
+// y32 = A x32 on the tensor cores (icc_op_apply_f32).
 int mixed_apply_f32(Op &op, const float *x, float *y) {
     int rc = mixed_init(op);
     if (rc) return rc;
@@ -437,6 +556,56 @@ int mixed_apply_f32(Op &op, const float *x, float *y) {
     return ICC_OK;
 }
 
+// x64 += sigma * xs32; xs32 = 0
+__global__ void ru_accumulate_kernel(long long n, double *__restrict__ x, float *__restrict__ xs, double sigma) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        x[i] += sigma * double(xs[i]);
+        xs[i] = 0.f;
+    }
+}
+
+// r32 = r64 / sigma (the FP64 residual replaces the FP32 recurrence residual); partials r'z, r'r
+__global__ void __launch_bounds__(kVecThreads)
+ru_replace_kernel(long long n, const double *__restrict__ r64, double inv_sigma, const float *__restrict__ inv,
+                  float *__restrict__ r32, double *__restrict__ partials) {
+    double rz = 0.0, rr = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float ri = float(r64[i] * inv_sigma);
+        r32[i] = ri;
+        rz += double(ri) * double(inv[i] * ri);
+        rr += double(ri) * double(ri);
+    }
+    rz = block_sum(rz);
+    rr = block_sum(rr);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = rz;
+        partials[2 * blockIdx.x + 1] = rr;
+    }
+}
+
+// continue the FP32 iteration from the replaced residual, keeping the search direction
+__global__ void __launch_bounds__(kVecThreads)
+ru_replace_finalize(const double *__restrict__ partials, int np, PcgState *st) {
+    double rz = 0.0, rr = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        rz += partials[2 * i];
+        rr += partials[2 * i + 1];
+    }
+    rz = block_sum(rz);
+    rr = block_sum(rr);
+    if (threadIdx.x == 0) {
+        st->rz_old = rz;
+        st->rel_res = sqrt(rr) / st->norm_b;
+        st->status = 0;
+    }
+}
+
+// Mixed-precision PCG with reliable updates (residual replacement): the Jacobi-PCG recurrence runs
+// in FP32 on the tensor-core operator; whenever its residual has fallen by `delta` since the last
+// replacement (or below tol), the FP32 solution increment is folded into the FP64 solution, the
+// true residual b - A x is recomputed with the FP64 operator, and the FP32 residual is replaced by
+// it while the search direction is kept.  Stops when the FP64 residual meets tol (the reference's
+// stopping rule, rust/src/solver.rs:56-58, evaluated on the true residual).
 int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter, const icc_solve_opts &opts,
                 double *x_out, int64_t *iters, double *rel_res) {
     int rc = op.ensure_pcg_buffers();
@@ -445,9 +614,10 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     MixedState &ms = *op.mixed;
     const int vb = op.vec_blocks;
     const long long n = op.ndof;
-    const double inner_tol = opts.inner_tol > 0.0 ? opts.inner_tol : 1e-3;
-    const int max_outer = opts.max_outer > 0 ? opts.max_outer : 60;
+    const double delta = opts.inner_tol > 0.0 ? opts.inner_tol : 0.1;
+    const int max_updates = opts.max_outer > 0 ? opts.max_outer : 1000;
     const int check_every = opts.check_every > 0 ? opts.check_every : 32;
+    const uint8_t *pm = op.mask_mode == ICC_MASK_ZERO ? op.d_mask : nullptr;
     int64_t launches = 0;
 
     if (!diag) {
@@ -462,7 +632,18 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     ICC_CUDA(cudaMemcpyAsync(ms.h_scalars, ms.d_scalars, 8, cudaMemcpyDeviceToHost, op.stream), "scalars");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "mixed init");
     const double nb = std::fmax(std::sqrt(ms.h_scalars[0]), 1e-16);
-    double rr = ms.h_scalars[0];
+    const double sigma = nb;  // FP32 quantities are scaled by 1 / |b|
+    if (max_iter == 0) {
+        ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
+        *iters = 0;
+        *rel_res = 1.0;
+        return ICC_NOT_CONVERGED;
+    }
+    ir_to_f32_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r64, ms.d_rhs32, ms.d_scalars);
+    pcg_init_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_rhs32, ms.d_inv32, ms.d_x32, ms.d_r32, ms.d_p32,
+                                                              op.d_partials, pm);
+    pcg_init_finalize<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state, tol, (long long)max_iter);
+    launches += 3;
 
     if (!ms.graph || ms.graph_batch != check_every) {
         if (ms.graph) cudaGraphExecDestroy(ms.graph);
@@ -477,70 +658,69 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         ms.graph_batch = check_every;
     }
 
-    int64_t total_inner = 0, outer = 0, fp64_applies = 0;
-    double res = std::sqrt(rr) / nb, prev_res = INFINITY;
     int status = ICC_NOT_CONVERGED;
-    int stall = 0;
+    int64_t updates = 0, launched = 0;
+    double res = 1.0, res_at_update = 1.0, best = INFINITY;
+    int no_progress = 0;
     for (;;) {
-        res = std::sqrt(rr) / nb;
-        if (res < tol) {
-            status = ICC_OK;
-            break;
+        ICC_CUDA(cudaGraphLaunch(ms.graph, op.stream), "graph launch");
+        launches += 6 * int64_t(check_every);
+        launched += check_every;
+        ICC_CUDA(cudaMemcpyAsync(ms.h_state, ms.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, op.stream), "state");
+        ICC_CUDA(cudaStreamSynchronize(op.stream), "inner sync");
+        const PcgState hs = *ms.h_state;
+        const bool stopped = hs.status != 0;
+        if (!stopped && !(hs.rel_res < delta * res_at_update)) {
+            if (launched > max_iter + 2 * int64_t(check_every))
+                return set_error(ICC_TIMEOUT, "mixed solve: device state did not reach a stop condition");
+            continue;
         }
-        if (!std::isfinite(res)) {
-            status = set_error(ICC_NAN, "mixed solve: non-finite residual");
-            break;
-        }
-        if (outer >= max_outer || total_inner >= max_iter) break;
-        if (res > 0.5 * prev_res) {
-            if (++stall >= 3) break;  // refinement no longer contracts: report NOT_CONVERGED
-        } else {
-            stall = 0;
-        }
-        prev_res = res;
-        // inner FP32 PCG on A d = r / |r|
-        ir_to_f32_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r64, ms.d_rhs32, ms.d_scalars);
-        pcg_init_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_rhs32, ms.d_inv32, ms.d_x32, ms.d_r32,
-                                                                  ms.d_p32, op.d_partials);
-        pcg_init_finalize<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state, inner_tol,
-                                                            (long long)(max_iter - total_inner));
-        launches += 3;
-        for (;;) {
-            ICC_CUDA(cudaMemcpyAsync(ms.h_state, ms.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, op.stream),
-                     "state");
-            ICC_CUDA(cudaStreamSynchronize(op.stream), "inner sync");
-            if (ms.h_state->status != 0) break;
-            ICC_CUDA(cudaGraphLaunch(ms.graph, op.stream), "graph launch");
-            launches += 6 * int64_t(check_every);
-        }
-        int err = 0;
-        ICC_CUDA(cudaMemcpy(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost), "err");
-        if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
-        if (ms.h_state->status == kStatNan) {
-            status = set_error(ICC_NAN, "mixed solve: non-finite inner reduction");
-            break;
-        }
-        total_inner += ms.h_state->iter;
-        // x += |r| d;  r = b - A x (FP64)
-        ir_update_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_x64, ms.d_x32, ms.d_scalars);
+        // reliable update: x += sigma xs; r = b - A x in FP64
+        ru_accumulate_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_x64, ms.d_x32, sigma);
         op.enqueue_apply(ms.d_x64, ms.d_y64, nullptr, nullptr);
         ir_residual_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, b, ms.d_y64, ms.d_r64, op.d_partials);
         sum_partials_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_scalars, 0);
         launches += 5;
         ICC_CUDA(cudaMemcpyAsync(ms.h_scalars, ms.d_scalars, 8, cudaMemcpyDeviceToHost, op.stream), "scalars");
-        ICC_CUDA(cudaStreamSynchronize(op.stream), "outer sync");
-        rr = ms.h_scalars[0];
-        outer++;
-        fp64_applies++;
+        ICC_CUDA(cudaStreamSynchronize(op.stream), "update sync");
+        updates++;
+        res = std::sqrt(ms.h_scalars[0]) / nb;
+        if (res < tol) {
+            status = ICC_OK;
+            break;
+        }
+        if (!std::isfinite(res) || hs.status == kStatNan) {
+            status = set_error(ICC_NAN, "mixed solve: non-finite residual");
+            break;
+        }
+        if (hs.status == kStatBreakdown) {
+            status = ICC_BREAKDOWN;
+            break;
+        }
+        if (hs.status == kStatMaxIter || hs.iter >= max_iter || updates >= max_updates) break;
+        if (res < 0.9 * best) {
+            best = res;
+            no_progress = 0;
+        } else if (++no_progress >= 8) {
+            break;  // FP32 recurrence no longer reduces the true residual: NOT_CONVERGED
+        }
+        ru_replace_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r64, 1.0 / sigma, ms.d_inv32, ms.d_r32,
+                                                             op.d_partials);
+        ru_replace_finalize<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
+        launches += 2;
+        res_at_update = res;
     }
+    int err = 0;
+    ICC_CUDA(cudaMemcpy(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
     ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
-    *iters = total_inner;
+    *iters = ms.h_state->iter;
     *rel_res = res;
-    op.last_info.iterations = total_inner;
-    op.last_info.outer_iterations = outer;
+    op.last_info.iterations = ms.h_state->iter;
+    op.last_info.outer_iterations = updates;
     op.last_info.rel_res = res;
-    op.last_info.fp64_applies = fp64_applies;
-    op.last_info.mixed_applies = total_inner;
+    op.last_info.fp64_applies = updates;
+    op.last_info.mixed_applies = ms.h_state->iter;
     op.last_info.kernel_launches = launches;
     return status;
 }

@@ -76,16 +76,18 @@ __global__ void inv_diag_kernel(long long n, const double *__restrict__ d, T *__
 }
 
 // x = 0, r = b, z = D^-1 r, p = z; partials: r'z and b'b   (rust/src/solver.rs:15-36)
+// pmask != null keeps p zero on fixed DOFs (the mixed form's inner loop, ICC_MASK_ZERO)
 template <class T>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_init_kernel(long long n, const T *__restrict__ b, const T *__restrict__ inv, T *__restrict__ x,
-                T *__restrict__ r, T *__restrict__ p, double *__restrict__ partials) {
+                T *__restrict__ r, T *__restrict__ p, double *__restrict__ partials,
+                const uint8_t *__restrict__ pmask = nullptr) {
     double rz = 0.0, bb = 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         T bi = b[i], zi = inv[i] * bi;
         x[i] = T(0);
         r[i] = bi;
-        p[i] = zi;
+        p[i] = (pmask && !pmask[i]) ? T(0) : zi;
         rz += double(bi) * double(zi);
         bb += double(bi) * double(bi);
     }
@@ -134,11 +136,11 @@ pcg_update_kernel(long long n, const T *__restrict__ p, const T *__restrict__ ap
 template <class T>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_p_kernel(long long n, const T *__restrict__ r, const T *__restrict__ inv, T *__restrict__ p,
-             const PcgState *__restrict__ st) {
+             const PcgState *__restrict__ st, const uint8_t *__restrict__ pmask = nullptr) {
     if (st->status != 0) return;
     const T beta = T(st->beta);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        p[i] = inv[i] * r[i] + beta * p[i];
+        p[i] = (pmask && !pmask[i]) ? T(0) : inv[i] * r[i] + beta * p[i];
 }
 
 }  // namespace icc
