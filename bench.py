@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-ref-solution", action="store_true", help="skip the tight FP64 error reference")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only run warmup + steps operator applies (for profiler captures)")
+    ap.add_argument("--delta", type=float, default=0.0,
+                    help="mixed form: FP64 residual replacement when the FP32 residual fell by this factor")
+    ap.add_argument("--check-every", type=int, default=32, help="PCG iterations per device batch")
     return ap.parse_args()
 
 
@@ -214,7 +217,7 @@ def run_ours(args):
     x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     precision = icc.MIXED if args.mode == "mixed" else icc.FP64
-    solver = icc.PcgSolver(20 * n, TOL, precision=precision)
+    solver = icc.PcgSolver(20 * n, TOL, precision=precision, check_every=args.check_every, inner_tol=args.delta)
 
     def barrier():
         if world > 1:
@@ -222,16 +225,18 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     if args.kernel_only:
-        y_dev = torch.empty_like(x_dev)
-        p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev)
+        vdt = torch.float32 if args.mode == "mixed" else torch.float64
+        apply = op.matvec_f32_dev if args.mode == "mixed" else op.matvec_dev
+        y_dev = torch.empty(n, dtype=vdt, device=dev)
+        p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev).to(vdt)
         for _ in range(args.warmup):
-            op.matvec_dev(p_dev.data_ptr(), y_dev.data_ptr())
+            apply(p_dev.data_ptr(), y_dev.data_ptr())
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             e0.record(stream)
         for _ in range(args.steps):
-            op.matvec_dev(p_dev.data_ptr(), y_dev.data_ptr())
+            apply(p_dev.data_ptr(), y_dev.data_ptr())
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()

@@ -42,6 +42,7 @@ struct Geom {
 
 struct PcgState {
     double rz_old, p_ap, alpha, beta, norm_b, rel_res, tol;
+    double rz_prev;        // r'z used by the last alpha (the beta of a residual replacement needs it)
     long long iter, max_iter;
     int status, pad;
 };

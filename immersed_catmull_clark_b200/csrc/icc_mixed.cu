@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "icc_device.cuh"
@@ -164,16 +165,24 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         const int m = tid;
         const int lx = m % kBX, ly = (m / kBX) % kBY, lz = m / (kBX * kBY);
         const int base = (lz * kPY + ly) * kPX + lx;
+        // patch rows (c, pz, py) of kPX floats; thread m < 108 copies row m
         auto load_patch = [&](int b, float *dst) {
-            BrickBox bb = brick_box(g, b);
-            for (int i = m; i < 3 * kPVol; i += 128) {
-                int c = i / kPVol, r = i - c * kPVol;
-                int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
-                int gx = bb.x0 + px, gy = bb.y0 + py, gz = bb.z0 + pz;
-                if (gx < g.cx && gy < g.cy && gz < g.cz)
-                    tc::cp_async4(dst + i, x + ((long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + gx));
-                else
-                    dst[i] = 0.f;
+            if (m < 3 * kPZ * kPY) {
+                const BrickBox bb = brick_box(g, b);
+                const int c = m / (kPZ * kPY), py = m % kPY, pz = (m / kPY) % kPZ;
+                const int gy = bb.y0 + py, gz = bb.z0 + pz;
+                float *drow = dst + m * kPX;
+                if (gy < g.cy && gz < g.cz) {
+                    const float *srow = x + (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
+#pragma unroll
+                    for (int px = 0; px < kPX; ++px) {
+                        if (bb.x0 + px < g.cx) tc::cp_async4(drow + px, srow + px);
+                        else drow[px] = 0.f;
+                    }
+                } else {
+#pragma unroll
+                    for (int px = 0; px < kPX; ++px) drow[px] = 0.f;
+                }
             }
             tc::cp_async_commit();
         };
@@ -201,13 +210,18 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             tc::fence_after_sync();
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n;
             const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kColSlot);
-#pragma unroll 1
+            const float *Pm = P + base;
+#pragma unroll
             for (int c8 = 0; c8 < kTcK / 8; ++c8) {
                 float hi[8], lo[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                    const int off = s_koff[c8 * 8 + q];
-                    const float v = (valid && off >= 0) ? P[off + base] : 0.f;
+                    const int k = c8 * 8 + q;  // compile-time: the patch offset folds to an immediate
+                    float v = 0.f;
+                    if (k < 81) {
+                        const int c = k / 27, a = k % 27;
+                        if (valid) v = Pm[c * kPVol + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
+                    }
                     hi[q] = tc::to_tf32(v);
                     lo[q] = tc::to_tf32(v - hi[q]);
                 }
@@ -267,20 +281,33 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                 for (int n = 0; n < 81; ++n) sY[r * 81 + n] = res[n];
             }
             tc::named_sync(2, 128);
-            float *outb = patch_out + (size_t)b * 3 * kPVol;
-            for (int i = et; i < 3 * kPVol; i += 128) {
-                int c = i / kPVol, rem = i - c * kPVol;
-                int px = rem % kPX, py = (rem / kPX) % kPY, pz = rem / (kPX * kPY);
-                float sum = 0.f;
-                if (px < bb.ex_n + 2 && py < bb.ey_n + 2 && pz < bb.ez_n + 2) {
-                    for (int qz = max(pz - 2, 0); qz <= min(pz, bb.ez_n - 1); ++qz)
-                        for (int qy = max(py - 2, 0); qy <= min(py, bb.ey_n - 1); ++qy)
-                            for (int qx = max(px - 2, 0); qx <= min(px, bb.ex_n - 1); ++qx) {
-                                int e = qx + kBX * (qy + kBY * qz);
-                                sum += sY[e * 81 + c * 27 + (px - qx) + 3 * (py - qy) + 9 * (pz - qz)];
+            // node sums: thread et < 108 owns patch row (c, pz, py) and accumulates its kPX nodes
+            if (et < 3 * kPZ * kPY) {
+                const int c = et / (kPZ * kPY), py = et % kPY, pz = (et / kPY) % kPZ;
+                float acc[kPX];
+#pragma unroll
+                for (int px = 0; px < kPX; ++px) acc[px] = 0.f;
+                if (py < bb.ey_n + 2 && pz < bb.ez_n + 2) {
+                    for (int dz = 0; dz < 3; ++dz) {
+                        const int qz = pz - dz;
+                        if (qz < 0 || qz >= bb.ez_n) continue;
+                        for (int dy = 0; dy < 3; ++dy) {
+                            const int qy = py - dy;
+                            if (qy < 0 || qy >= bb.ey_n) continue;
+                            const float *Yr = sY + (kBX * (qy + kBY * qz)) * 81 + c * 27 + 3 * dy + 9 * dz;
+#pragma unroll
+                            for (int qx = 0; qx < kBX; ++qx) {
+                                if (qx < bb.ex_n) {
+#pragma unroll
+                                    for (int dx = 0; dx < 3; ++dx) acc[qx + dx] += Yr[qx * 81 + dx];
+                                }
                             }
+                        }
+                    }
                 }
-                outb[i] = sum;
+                float *orow = patch_out + (size_t)b * 3 * kPVol + et * kPX;
+#pragma unroll
+                for (int px = 0; px < kPX; ++px) orow[px] = acc[px];
             }
         }
     } else if (lane == 0) {
@@ -535,12 +562,12 @@ static void enqueue_inner_iteration(Op &op) {
     const int vb = op.vec_blocks;
     const bool pre = op.mask_mode == ICC_MASK_ZERO;
     const uint8_t *pm = pre ? op.d_mask : nullptr;
+    pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state, pm);
     enqueue_apply_tc(op, ms.d_p32, ms.d_ap32, op.d_partials, ms.d_state, pre);
     pcg_alpha_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
     pcg_update_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_p32, ms.d_ap32, ms.d_inv32, ms.d_x32,
                                                                 ms.d_r32, op.d_partials, ms.d_state);
     pcg_beta_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
-    pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state, pm);
 }
 
 // y32 = A x32 on the tensor cores (icc_op_apply_f32).
@@ -583,7 +610,8 @@ ru_replace_kernel(long long n, const double *__restrict__ r64, double inv_sigma,
     }
 }
 
-// continue the FP32 iteration from the replaced residual, keeping the search direction
+// continue the FP32 iteration from the replaced residual: the next search direction is
+// p = z + beta p with beta = r'z (replaced) / r'z (of the last alpha), as a reliable update does
 __global__ void __launch_bounds__(kVecThreads)
 ru_replace_finalize(const double *__restrict__ partials, int np, PcgState *st) {
     double rz = 0.0, rr = 0.0;
@@ -594,6 +622,7 @@ ru_replace_finalize(const double *__restrict__ partials, int np, PcgState *st) {
     rz = block_sum(rz);
     rr = block_sum(rr);
     if (threadIdx.x == 0) {
+        st->beta = rz / st->rz_prev;
         st->rz_old = rz;
         st->rel_res = sqrt(rr) / st->norm_b;
         st->status = 0;
@@ -690,7 +719,10 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
             break;
         }
         if (!std::isfinite(res) || hs.status == kStatNan) {
-            status = set_error(ICC_NAN, "mixed solve: non-finite residual");
+            status = set_error(ICC_NAN, "mixed solve: non-finite residual (FP64 " + std::to_string(res) +
+                                            ", FP32 " + std::to_string(hs.rel_res) + ", p'Ap " +
+                                            std::to_string(hs.p_ap) + ", iteration " + std::to_string(hs.iter) +
+                                            ", update " + std::to_string(updates) + ")");
             break;
         }
         if (hs.status == kStatBreakdown) {

@@ -205,6 +205,7 @@ pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, dou
         st->max_iter = max_iter;
         st->status = max_iter > 0 ? 0 : kStatMaxIter;
         st->alpha = st->beta = st->p_ap = 0.0;
+        st->rz_prev = rz;
     }
 }
 
@@ -233,6 +234,7 @@ __global__ void __launch_bounds__(kVecThreads) pcg_beta_kernel(const double *__r
     if (threadIdx.x == 0) {
         double res = sqrt(rr) / st->norm_b;
         st->rel_res = res;
+        st->rz_prev = st->rz_old;  // the r'z of this iteration's alpha
         if (res < st->tol) {
             st->status = kStatConverged;
         } else if (!isfinite(res)) {
@@ -435,14 +437,16 @@ int Op::ensure_pcg_buffers() {
     return ICC_OK;
 }
 
-// One PCG iteration (rust/src/solver.rs:40-72) as six launches; every kernel returns at once
-// when the state says the solve has finished, so a batch may overrun harmlessly.
+// One PCG iteration (rust/src/solver.rs:40-72) as six launches: p = z + beta p (beta = 0 on the
+// first iteration, so p = z), Ap, alpha, x/r update, convergence test and the next beta.  Every
+// kernel returns at once when the state says the solve has finished, so a batch may overrun
+// harmlessly.
 void Op::enqueue_pcg_iteration() {
+    pcg_p_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_r, d_inv, d_p, d_state);
     enqueue_apply(d_p, d_ap, d_partials, d_state);
     pcg_alpha_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
     pcg_update_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials, d_state);
     pcg_beta_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
-    pcg_p_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_r, d_inv, d_p, d_state);
 }
 
 int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_iter, int check_every, double *x,
