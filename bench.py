@@ -217,7 +217,9 @@ def run_ours(args):
     x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     precision = icc.MIXED if args.mode == "mixed" else icc.FP64
-    solver = icc.PcgSolver(20 * n, TOL, precision=precision, check_every=args.check_every, inner_tol=args.delta)
+    # iteration cap: 20 n as the reference's solve_state, but at most 100k for the benchmark
+    solver = icc.PcgSolver(min(20 * n, 100000), TOL, precision=precision, check_every=args.check_every,
+                           inner_tol=args.delta)
 
     def barrier():
         if world > 1:

@@ -688,7 +688,8 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     }
 
     int status = ICC_NOT_CONVERGED;
-    int64_t updates = 0, launched = 0;
+    int64_t updates = 0, launched = 0, iter_at_update = 0;
+    constexpr int64_t kMaxSegment = 512;  // FP32 iterations between residual replacements at most
     double res = 1.0, res_at_update = 1.0, best = INFINITY;
     int no_progress = 0;
     for (;;) {
@@ -699,11 +700,16 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         ICC_CUDA(cudaStreamSynchronize(op.stream), "inner sync");
         const PcgState hs = *ms.h_state;
         const bool stopped = hs.status != 0;
-        if (!stopped && !(hs.rel_res < delta * res_at_update)) {
+        // replace the residual when the FP32 recurrence has gained delta, or after a bounded
+        // segment: an FP32 recurrence stalls once its drift from the true residual reaches the
+        // gain it is asked for, so a stalled segment must not run on
+        const bool seg_full = hs.iter - iter_at_update >= kMaxSegment;
+        if (!stopped && !seg_full && !(hs.rel_res < delta * res_at_update)) {
             if (launched > max_iter + 2 * int64_t(check_every))
                 return set_error(ICC_TIMEOUT, "mixed solve: device state did not reach a stop condition");
             continue;
         }
+        iter_at_update = hs.iter;
         // reliable update: x += sigma xs; r = b - A x in FP64
         ru_accumulate_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_x64, ms.d_x32, sigma);
         op.enqueue_apply(ms.d_x64, ms.d_y64, nullptr, nullptr);
