@@ -67,6 +67,7 @@ struct Op {
     double *d_x = nullptr, *d_r = nullptr, *d_p = nullptr, *d_ap = nullptr, *d_inv = nullptr, *d_b = nullptr,
            *d_diag = nullptr, *d_partials = nullptr;
     PcgState *d_state = nullptr, *h_state = nullptr;
+    unsigned *d_counter = nullptr;          // last-CTA counter of the fused reductions
     cudaGraphExec_t graph_exec = nullptr;
     int graph_batch = 0;
     icc_solve_info last_info{};

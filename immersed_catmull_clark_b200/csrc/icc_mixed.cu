@@ -281,33 +281,30 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                 for (int n = 0; n < 81; ++n) sY[r * 81 + n] = res[n];
             }
             tc::named_sync(2, 128);
-            // node sums: thread et < 108 owns patch row (c, pz, py) and accumulates its kPX nodes
-            if (et < 3 * kPZ * kPY) {
-                const int c = et / (kPZ * kPY), py = et % kPY, pz = (et / kPY) % kPZ;
-                float acc[kPX];
+            // node sums: a warp task is 3 patch rows; lane = (row, px) sums the <= 27 element
+            // contributions of one node, lanes along x hit distinct banks (element stride 81)
+            if (lane < 3 * kPX) {
+                const int lrow = lane / kPX, px = lane % kPX;
+                const bool okx0 = px < bb.ex_n, okx1 = px >= 1 && px - 1 < bb.ex_n, okx2 = px >= 2 && px - 2 < bb.ex_n;
+                for (int task = q4; task < kPZ * kPY; task += 4) {
+                    const int row = task * 3 + lrow;   // 0 .. 107 = (c, pz, py)
+                    const int c = row / (kPZ * kPY), py = row % kPY, pz = (row / kPY) % kPZ;
+                    const bool oky[3] = {py < bb.ey_n, py >= 1 && py - 1 < bb.ey_n, py >= 2 && py - 2 < bb.ey_n};
+                    const bool okz[3] = {pz < bb.ez_n, pz >= 1 && pz - 1 < bb.ez_n, pz >= 2 && pz - 2 < bb.ez_n};
+                    const bool okx[3] = {okx0, okx1, okx2};
+                    // element (px-dx, py-dy, pz-dz), local DOF c*27 + dx + 3 dy + 9 dz
+                    const float *Yb = sY + (px + kBX * (py + kBY * pz)) * 81 + c * 27;
+                    float sum = 0.f;
 #pragma unroll
-                for (int px = 0; px < kPX; ++px) acc[px] = 0.f;
-                if (py < bb.ey_n + 2 && pz < bb.ez_n + 2) {
-                    for (int dz = 0; dz < 3; ++dz) {
-                        const int qz = pz - dz;
-                        if (qz < 0 || qz >= bb.ez_n) continue;
-                        for (int dy = 0; dy < 3; ++dy) {
-                            const int qy = py - dy;
-                            if (qy < 0 || qy >= bb.ey_n) continue;
-                            const float *Yr = sY + (kBX * (qy + kBY * qz)) * 81 + c * 27 + 3 * dy + 9 * dz;
+                    for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
-                            for (int qx = 0; qx < kBX; ++qx) {
-                                if (qx < bb.ex_n) {
+                        for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
-                                    for (int dx = 0; dx < 3; ++dx) acc[qx + dx] += Yr[qx * 81 + dx];
-                                }
-                            }
-                        }
-                    }
+                            for (int dx = 0; dx < 3; ++dx)
+                                if (okz[dz] && oky[dy] && okx[dx])
+                                    sum += Yb[-(dx + kBX * (dy + kBY * dz)) * 81 + dx + 3 * dy + 9 * dz];
+                    patch_out[(size_t)b * 3 * kPVol + row * kPX + px] = sum;
                 }
-                float *orow = patch_out + (size_t)b * 3 * kPVol + et * kPX;
-#pragma unroll
-                for (int px = 0; px < kPX; ++px) orow[px] = acc[px];
             }
         }
     } else if (lane == 0) {
@@ -322,10 +319,12 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
             const int s = it & 1;
-            pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
             const int p0 = pass_start[b], p1 = pass_start[b + 1];
+            int t_next = pass_type[p0];
+            pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
             for (int pi = p0; pi < p1; ++pi, ++j) {
-                const int t = pass_type[pi];
+                const int t = t_next;
+                if (pi + 1 < p1) t_next = pass_type[pi + 1];
                 // the previous pass has been drained: no MMA still reads D or a B buffer
                 if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
                 int buf = 0;
@@ -562,12 +561,17 @@ static void enqueue_inner_iteration(Op &op) {
     const int vb = op.vec_blocks;
     const bool pre = op.mask_mode == ICC_MASK_ZERO;
     const uint8_t *pm = pre ? op.d_mask : nullptr;
+    const int grid = std::min(op.num_sms, op.g.nbricks);
     pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state, pm);
-    enqueue_apply_tc(op, ms.d_p32, ms.d_ap32, op.d_partials, ms.d_state, pre);
-    pcg_alpha_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(
+        op.g, ms.d_p32, op.d_mask, (op.mask_mode != ICC_MASK_NONE && !pre) ? 1 : 0, ms.d_scale32, op.d_type_id,
+        ms.d_bmat, ms.main_type, ms.d_pass_start, ms.d_pass_type, ms.d_patch32, ms.d_err, ms.d_state);
+    gather_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, ms.d_p32, op.d_mask, op.mask_mode,
+                                                            ms.d_ap32, op.d_partials, ms.d_state, ms.d_state,
+                                                            op.d_counter);
     pcg_update_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_p32, ms.d_ap32, ms.d_inv32, ms.d_x32,
-                                                                ms.d_r32, op.d_partials, ms.d_state);
-    pcg_beta_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
+                                                                ms.d_r32, op.d_partials, ms.d_state, ms.d_state,
+                                                                op.d_counter);
 }
 
 // y32 = A x32 on the tensor cores (icc_op_apply_f32).
@@ -694,7 +698,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     int no_progress = 0;
     for (;;) {
         ICC_CUDA(cudaGraphLaunch(ms.graph, op.stream), "graph launch");
-        launches += 6 * int64_t(check_every);
+        launches += 4 * int64_t(check_every);
         launched += check_every;
         ICC_CUDA(cudaMemcpyAsync(ms.h_state, ms.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, op.stream), "state");
         ICC_CUDA(cudaStreamSynchronize(op.stream), "inner sync");

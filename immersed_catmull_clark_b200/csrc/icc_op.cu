@@ -214,12 +214,7 @@ __global__ void __launch_bounds__(kVecThreads) pcg_alpha_kernel(const double *__
     double s = 0.0;
     for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
     s = block_sum(s);
-    if (threadIdx.x == 0) {
-        st->iter += 1;
-        st->p_ap = s;
-        if (!(s > 0.0)) st->status = isfinite(s) ? kStatBreakdown : kStatNan;
-        else st->alpha = st->rz_old / s;
-    }
+    if (threadIdx.x == 0) pcg_alpha_step(st, s);
 }
 
 __global__ void __launch_bounds__(kVecThreads) pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st) {
@@ -231,20 +226,7 @@ __global__ void __launch_bounds__(kVecThreads) pcg_beta_kernel(const double *__r
     }
     rr = block_sum(rr);
     rz = block_sum(rz);
-    if (threadIdx.x == 0) {
-        double res = sqrt(rr) / st->norm_b;
-        st->rel_res = res;
-        st->rz_prev = st->rz_old;  // the r'z of this iteration's alpha
-        if (res < st->tol) {
-            st->status = kStatConverged;
-        } else if (!isfinite(res)) {
-            st->status = kStatNan;
-        } else {
-            st->beta = rz / st->rz_old;
-            st->rz_old = rz;
-            if (st->iter >= st->max_iter) st->status = kStatMaxIter;
-        }
-    }
+    if (threadIdx.x == 0) pcg_beta_step(st, rr, rz);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -262,7 +244,7 @@ static int dev_alloc(T **p, size_t count, const char *what) {
 Op::~Op() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     void *bufs[] = {d_x_in, d_y_out, d_scale, d_kfrag, d_kdiag, d_type_id, d_tile_start, d_tile_type, d_tile_elem,
-                    d_mask, d_patch, d_x, d_r, d_p, d_ap, d_inv, d_b, d_diag, d_partials, d_state};
+                    d_mask, d_patch, d_x, d_r, d_p, d_ap, d_inv, d_b, d_diag, d_partials, d_state, d_counter};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_state) cudaFreeHost(h_state);
@@ -368,6 +350,8 @@ int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type
     vec_blocks = num_sms * 4;
     if ((rc = dev_alloc(&d_partials, (size_t)vec_blocks * 2, "alloc partials"))) return rc;
     if ((rc = dev_alloc(&d_state, 1, "alloc state"))) return rc;
+    if ((rc = dev_alloc(&d_counter, 1, "alloc counter"))) return rc;
+    ICC_CUDA(cudaMemset(d_counter, 0, sizeof(unsigned)), "clear counter");
     ICC_CUDA(cudaMallocHost((void **)&h_state, sizeof(PcgState)), "alloc pinned state");
     ICC_CUDA(cudaFuncSetAttribute(apply_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem),
              "cudaFuncSetAttribute");
@@ -443,10 +427,13 @@ int Op::ensure_pcg_buffers() {
 // harmlessly.
 void Op::enqueue_pcg_iteration() {
     pcg_p_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_r, d_inv, d_p, d_state);
-    enqueue_apply(d_p, d_ap, d_partials, d_state);
-    pcg_alpha_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
-    pcg_update_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials, d_state);
-    pcg_beta_kernel<<<1, kVecThreads, 0, stream>>>(d_partials, vec_blocks, d_state);
+    apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
+        g, d_p, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
+        d_state);
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, d_p, d_mask, mask_mode, d_ap, d_partials,
+                                                                  d_state, d_state, d_counter);
+    pcg_update_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials,
+                                                                      d_state, d_state, d_counter);
 }
 
 int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_iter, int check_every, double *x,
@@ -485,7 +472,7 @@ int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_it
             return set_error(ICC_TIMEOUT, "pcg: device state did not reach a stop condition");
         ICC_CUDA(cudaGraphLaunch(graph_exec, stream), "graph launch");
         launched += check_every;
-        launches += 6 * int64_t(check_every);
+        launches += 4 * int64_t(check_every);
     }
     ICC_CUDA(cudaMemcpyAsync(x, d_x, (size_t)ndof * 8, cudaMemcpyDeviceToDevice, stream), "copy x");
     *iters = h_state->iter;

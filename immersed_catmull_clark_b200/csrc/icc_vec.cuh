@@ -25,12 +25,55 @@ __device__ __forceinline__ int node_bricks(int j, int B, int nb, int *bi, int *l
     return 1;
 }
 
+// ---- PCG scalar steps (rust/src/solver.rs:41-71), run by one thread ---------------------------
+
+// p'Ap -> alpha, or breakdown (rust/src/solver.rs:41-51)
+__device__ __forceinline__ void pcg_alpha_step(PcgState *st, double p_ap) {
+    st->iter += 1;
+    st->p_ap = p_ap;
+    if (!(p_ap > 0.0)) st->status = isfinite(p_ap) ? kStatBreakdown : kStatNan;
+    else st->alpha = st->rz_old / p_ap;
+}
+
+// relative residual test, then beta (rust/src/solver.rs:56-71)
+__device__ __forceinline__ void pcg_beta_step(PcgState *st, double rr, double rz) {
+    double res = sqrt(rr) / st->norm_b;
+    st->rel_res = res;
+    st->rz_prev = st->rz_old;  // the r'z of this iteration's alpha
+    if (res < st->tol) {
+        st->status = kStatConverged;
+    } else if (!isfinite(res)) {
+        st->status = kStatNan;
+    } else {
+        st->beta = rz / st->rz_old;
+        st->rz_old = rz;
+        if (st->iter >= st->max_iter) st->status = kStatMaxIter;
+    }
+}
+
+// True in exactly one CTA: the last to finish.  Every CTA has stored its partial before calling;
+// the last one then reads all partials (in fixed order, so the result does not depend on which
+// CTA is last) and resets the counter for the next use.
+__device__ __forceinline__ bool last_block(unsigned *counter) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        if (threadIdx.x == 0) *counter = 0u;
+    }
+    return is_last;
+}
+
 // y = sum of the brick partials of each node (fixed order), output mask applied;
-// optionally the CTA partial of p'y (in double).
+// optionally the CTA partial of p'y (in double), and with `fuse` the alpha step in the last CTA.
 template <class T>
 __global__ void __launch_bounds__(kVecThreads)
 gather_kernel(Geom g, const T *__restrict__ patch, const T *__restrict__ p, const uint8_t *__restrict__ mask,
-              int mask_mode, T *__restrict__ y, double *__restrict__ partials, const PcgState *__restrict__ st) {
+              int mask_mode, T *__restrict__ y, double *__restrict__ partials, const PcgState *st,
+              PcgState *fuse = nullptr, unsigned *counter = nullptr) {
     if (st && st->status != 0) return;
     double dot = 0.0;
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
@@ -64,6 +107,12 @@ gather_kernel(Geom g, const T *__restrict__ patch, const T *__restrict__ p, cons
     if (partials) {
         dot = block_sum(dot);
         if (threadIdx.x == 0) partials[blockIdx.x] = dot;
+        if (fuse && last_block(counter)) {
+            double s2 = 0.0;
+            for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) s2 += __ldcg(partials + i);
+            s2 = block_sum(s2);
+            if (threadIdx.x == 0) pcg_alpha_step(fuse, s2);
+        }
     }
 }
 
@@ -113,7 +162,7 @@ template <class T>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_update_kernel(long long n, const T *__restrict__ p, const T *__restrict__ ap, const T *__restrict__ inv,
                   T *__restrict__ x, T *__restrict__ r, double *__restrict__ partials,
-                  const PcgState *__restrict__ st) {
+                  const PcgState *st, PcgState *fuse = nullptr, unsigned *counter = nullptr) {
     if (st->status != 0) return;
     const T alpha = T(st->alpha);
     double rr = 0.0, rz = 0.0;
@@ -129,6 +178,16 @@ pcg_update_kernel(long long n, const T *__restrict__ p, const T *__restrict__ ap
     if (threadIdx.x == 0) {
         partials[2 * blockIdx.x] = rr;
         partials[2 * blockIdx.x + 1] = rz;
+    }
+    if (fuse && last_block(counter)) {
+        double a = 0.0, c = 0.0;
+        for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+            a += __ldcg(partials + 2 * i);
+            c += __ldcg(partials + 2 * i + 1);
+        }
+        a = block_sum(a);
+        c = block_sum(c);
+        if (threadIdx.x == 0) pcg_beta_step(fuse, a, c);
     }
 }
 
