@@ -70,25 +70,27 @@ struct MixedState {
 // ------------------------------------------------------------------------------------------
 
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
-// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles:
+// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (13 warps):
 //   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; split the current
 //     brick's gathered element vectors into TF32 hi/lo and store them as the A operand straight
 //     into TMEM (row m = element m = lane m), double-buffered in two A slots;
-//   warp 8 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
-//     element type, buffer 1 for the others, fetched with cp.async.bulk), issues the 33
-//     tcgen05.mma (A from TMEM, B from shared memory) per type pass into one TMEM accumulator;
-//   warps 4-7 (epilogue): drain the accumulator with tcgen05.ld, keep each row's own type pass,
-//     scale by s_e, stage the rows in shared memory and write the brick's patch partial sums.
-// mbarriers: a_full[2] (builders -> MMA), a_empty[2] (MMA commit -> builders), d_full (MMA commit
-// -> epilogue), d_empty (epilogue -> MMA), b_full[2] (bulk copies).  Every wait is bounded; on
-// time-out the CTA raises a shared abort flag, so all roles finish promptly and the host reports
-// ICC_TIMEOUT.
-constexpr int kPtThreads = 288;
+//   warp 12 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
+//     element type, buffer 1 for the others, fetched with cp.async.bulk and prefetched while a
+//     main-type pass runs), issues the 33 tcgen05.mma (A from TMEM, B from shared memory) per
+//     type pass into one TMEM accumulator;
+//   warps 4-7 (drain): read the accumulator with tcgen05.ld, keep each row's own type pass, scale
+//     by s_e and stage the brick's element results in shared memory (two staging buffers);
+//   warps 8-11 (sum): add up the staged results per patch node and write the brick partials.
+// mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), y_full/y_empty (staging
+// buffers), b_full/b1_free (B buffers).  Every wait is bounded; on time-out the CTA raises a shared
+// abort flag, so all roles finish promptly and the host reports ICC_TIMEOUT.
+constexpr int kPtThreads = 13 * 32;
 constexpr int kColSlot = 176;    // A slot s: hi at s*176 + [0,88), lo at s*176 + 88 + [0,88)
 constexpr int kColD = 352;       // accumulator: 96 columns
 constexpr uint32_t kPtTmemCols = 512;
-constexpr int kPtSmem = (4 * kBFl + 2 * 3 * kPVol + kEPB * 81) * 4;  // 185,280 B
-constexpr uint32_t kBBytes = 2 * kBFl * 4;                            // one type, hi + lo
+constexpr int kYFl = kEPB * 81;  // one staging buffer
+constexpr int kPtSmem = (4 * kBFl + 2 * 3 * kPVol + 2 * kYFl) * 4;  // 226,752 B
+constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // one type, hi + lo
 
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
     for (long long i = 0; i < kWaitLimit; ++i) {
@@ -116,6 +118,31 @@ __device__ __forceinline__ BrickBox brick_box(const Geom &g, int b) {
     return r;
 }
 
+// per-row data of one brick, loaded a brick ahead by the drain warps
+struct RowMeta {
+    int type, p0, p1, t0;
+    float scale;
+};
+
+__device__ __forceinline__ RowMeta row_meta(const Geom &g, int b, int r, const int *__restrict__ type_id,
+                                            const float *__restrict__ scale, const int *__restrict__ pass_start,
+                                            const int *__restrict__ pass_type) {
+    RowMeta m;
+    const BrickBox bb = brick_box(g, b);
+    const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
+    m.type = -1;
+    m.scale = 0.f;
+    if (lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n) {
+        long long eg = (long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz));
+        m.type = type_id[eg];
+        m.scale = scale[eg];
+    }
+    m.p0 = pass_start[b];
+    m.p1 = pass_start[b + 1];
+    m.t0 = pass_type[m.p0];
+    return m;
+}
+
 __global__ void __launch_bounds__(kPtThreads, 1)
 apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__ mask, int mask_in,
                 const float *__restrict__ scale, const int *__restrict__ type_id, const float4 *__restrict__ bmat,
@@ -125,22 +152,17 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [2 buffers][hi, lo][kBFl]
     float *sP = psm + 4 * kBFl;           // [2][3 * kPVol]
-    float *sY = sP + 2 * 3 * kPVol;       // [kEPB][81]
-    __shared__ __align__(8) uint64_t bars[8];
+    float *sYb = sP + 2 * 3 * kPVol;      // [2][kEPB][81]
+    __shared__ __align__(8) uint64_t bars[13];
     __shared__ uint32_t tmem_base;
-    __shared__ int s_koff[88];
     __shared__ volatile int s_abort;
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *b_full = bars + 6;
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *y_full = bars + 6,
+             *y_empty = bars + 8, *b_full = bars + 10, *b1_free = bars + 12;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
         tc::tmem_alloc(&tmem_base, kPtTmemCols);
         tc::tmem_relinquish();
-    }
-    if (tid < 88) {
-        int k = tid;
-        int c = k / 27, a = k % 27;
-        s_koff[tid] = k < 81 ? c * kPVol + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3 : -1;
     }
     if (tid == 0) {
         tc::mbar_init(&a_full[0], 128);
@@ -149,8 +171,13 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         tc::mbar_init(&a_empty[1], 1);
         tc::mbar_init(d_full, 1);
         tc::mbar_init(d_empty, 128);
+        tc::mbar_init(&y_full[0], 128);
+        tc::mbar_init(&y_full[1], 128);
+        tc::mbar_init(&y_empty[0], 128);
+        tc::mbar_init(&y_empty[1], 128);
         tc::mbar_init(&b_full[0], 1);
         tc::mbar_init(&b_full[1], 1);
+        tc::mbar_init(b1_free, 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
@@ -235,32 +262,26 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         }
         tc::cp_async_wait<0>();
     } else if (warp < 8) {
-        // ------------------------------ epilogue ------------------------------
+        // ------------------------------ drain ------------------------------
         const int q4 = warp & 3;
         const int r = q4 * 32 + lane;   // TMEM lane quadrant of this warp = its rows
-        const int et = tid - 128;       // 0..127 for the node sum
-        const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
         const uint32_t dcol = tmem + ((uint32_t)(q4 * 32) << 16) + kColD;
         int j = 0;
+        RowMeta next{};
+        if (nmine > 0) next = row_meta(g, blockIdx.x, r, type_id, scale, pass_start, pass_type);
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
-            const BrickBox bb = brick_box(g, b);
-            const bool valid = lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n;
-            int my_type = -1;
-            float se = 0.f;
-            if (valid) {
-                long long eg = (long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz));
-                my_type = type_id[eg];
-                se = scale[eg];
-            }
-            const int p0 = pass_start[b], p1 = pass_start[b + 1];
+            const RowMeta cur = next;
+            if (it + 1 < nmine) next = row_meta(g, b + gridDim.x, r, type_id, scale, pass_start, pass_type);
             float res[81];
 #pragma unroll
             for (int n = 0; n < 81; ++n) res[n] = 0.f;
-            for (int pi = p0; pi < p1; ++pi, ++j) {
-                const int t = pass_type[pi];
+            int t = cur.t0;
+            for (int pi = cur.p0; pi < cur.p1; ++pi, ++j) {
+                const int t_next = pi + 1 < cur.p1 ? pass_type[pi + 1] : -1;
                 pt_wait(d_full, uint32_t(j) & 1u, &s_abort, err);
                 tc::fence_after_sync();
+                const bool take = cur.type == t;
 #pragma unroll
                 for (int cc = 0; cc < kTcN / 16; ++cc) {
                     uint32_t rr[16];
@@ -269,29 +290,42 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
 #pragma unroll
                     for (int q = 0; q < 16; ++q) {
                         const int n = cc * 16 + q;
-                        if (n < 81 && my_type == t) res[n] = se * __uint_as_float(rr[q]);
+                        if (n < 81) res[n] = take ? cur.scale * __uint_as_float(rr[q]) : res[n];
                     }
                 }
                 tc::fence_before_sync();
                 tc::mbar_arrive(d_empty);
+                t = t_next;
             }
-            tc::named_sync(2, 128);   // the previous brick's node sum is done with sY
-            if (valid) {
+            const int y = it & 1;
+            if (it >= 2) pt_wait(&y_empty[y], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
+            if (cur.type >= 0) {
+                float *sY = sYb + y * kYFl;
 #pragma unroll
                 for (int n = 0; n < 81; ++n) sY[r * 81 + n] = res[n];
             }
-            tc::named_sync(2, 128);
-            // node sums: a warp task is 3 patch rows; lane = (row, px) sums the <= 27 element
-            // contributions of one node, lanes along x hit distinct banks (element stride 81)
-            if (lane < 3 * kPX) {
-                const int lrow = lane / kPX, px = lane % kPX;
-                const bool okx0 = px < bb.ex_n, okx1 = px >= 1 && px - 1 < bb.ex_n, okx2 = px >= 2 && px - 2 < bb.ex_n;
+            tc::mbar_arrive(&y_full[y]);
+        }
+    } else if (warp < 12) {
+        // ------------------------------ sum ------------------------------
+        const int q4 = warp & 3;
+        const bool active = lane < 3 * kPX;
+        const int lrow = lane / kPX, px = lane % kPX;
+        for (int it = 0; it < nmine; ++it) {
+            const int b = blockIdx.x + it * gridDim.x;
+            const int y = it & 1;
+            const BrickBox bb = brick_box(g, b);
+            pt_wait(&y_full[y], uint32_t(it >> 1) & 1u, &s_abort, err);
+            const float *sY = sYb + y * kYFl;
+            if (active) {
+                // a warp task is 3 patch rows; lane = (row, px) sums the <= 27 element contributions
+                // of one node; lanes along x hit distinct banks (element stride 81)
+                const bool okx[3] = {px < bb.ex_n, px >= 1 && px - 1 < bb.ex_n, px >= 2 && px - 2 < bb.ex_n};
                 for (int task = q4; task < kPZ * kPY; task += 4) {
                     const int row = task * 3 + lrow;   // 0 .. 107 = (c, pz, py)
                     const int c = row / (kPZ * kPY), py = row % kPY, pz = (row / kPY) % kPZ;
                     const bool oky[3] = {py < bb.ey_n, py >= 1 && py - 1 < bb.ey_n, py >= 2 && py - 2 < bb.ey_n};
                     const bool okz[3] = {pz < bb.ez_n, pz >= 1 && pz - 1 < bb.ez_n, pz >= 2 && pz - 2 < bb.ez_n};
-                    const bool okx[3] = {okx0, okx1, okx2};
                     // element (px-dx, py-dy, pz-dz), local DOF c*27 + dx + 3 dy + 9 dz
                     const float *Yb = sY + (px + kBX * (py + kBY * pz)) * 81 + c * 27;
                     float sum = 0.f;
@@ -306,6 +340,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                     patch_out[(size_t)b * 3 * kPVol + row * kPX + px] = sum;
                 }
             }
+            tc::mbar_arrive(&y_empty[y]);
         }
     } else if (lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
@@ -313,29 +348,37 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         tc::mbar_arrive_expect_tx(&b_full[0], kBBytes);
         tc::bulk_g2s(sB, bmat + (size_t)main_type * (2 * kBFl / 4), kBBytes, &b_full[0]);
         pt_wait(&b_full[0], 0u, &s_abort, err);
-        int tag1 = -1;
-        uint32_t b1_phase = 0;
+        int tag1 = -1;             // type held (or being fetched) in B buffer 1
+        bool pending = false;      // a fetch into buffer 1 has not been waited for yet
+        uint32_t b1_loads = 0, b1_uses = 0;
+        auto fetch1 = [&](int t) {
+            if (b1_uses > 0) pt_wait(b1_free, (b1_uses - 1) & 1u, &s_abort, err);  // no MMA reads buffer 1
+            tc::mbar_arrive_expect_tx(&b_full[1], kBBytes);
+            tc::bulk_g2s(sB + 2 * kBFl, bmat + (size_t)t * (2 * kBFl / 4), kBBytes, &b_full[1]);
+            tag1 = t;
+            pending = true;
+            b1_loads++;
+        };
         int j = 0;
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
             const int s = it & 1;
             const int p0 = pass_start[b], p1 = pass_start[b + 1];
-            int t_next = pass_type[p0];
+            const int bn = b + gridDim.x;
+            const int pn = it + 1 < nmine ? pass_start[bn] : -1;
+            int t = pass_type[p0];
             pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
             for (int pi = p0; pi < p1; ++pi, ++j) {
-                const int t = t_next;
-                if (pi + 1 < p1) t_next = pass_type[pi + 1];
-                // the previous pass has been drained: no MMA still reads D or a B buffer
+                const int t_next = pi + 1 < p1 ? pass_type[pi + 1] : (pn >= 0 ? pass_type[pn] : -1);
+                // the previous pass has been drained: no MMA still writes the accumulator
                 if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
                 int buf = 0;
                 if (t != main_type) {
                     buf = 1;
-                    if (tag1 != t) {
-                        tc::mbar_arrive_expect_tx(&b_full[1], kBBytes);
-                        tc::bulk_g2s(sB + 2 * kBFl, bmat + (size_t)t * (2 * kBFl / 4), kBBytes, &b_full[1]);
-                        pt_wait(&b_full[1], b1_phase & 1u, &s_abort, err);
-                        b1_phase++;
-                        tag1 = t;
+                    if (tag1 != t) fetch1(t);
+                    if (pending) {
+                        pt_wait(&b_full[1], (b1_loads - 1) & 1u, &s_abort, err);
+                        pending = false;
                     }
                 }
                 tc::fence_after_sync();
@@ -351,10 +394,19 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                     tc::mma_tf32_ts(tmem + kColD, ah, dbh, idesc, 1u);
                 }
                 tc::mma_commit(d_full);
+                if (buf == 1) {
+                    tc::mma_commit(b1_free);
+                    b1_uses++;
+                } else if (t_next >= 0 && t_next != main_type && t_next != tag1) {
+                    fetch1(t_next);  // overlaps this main-type pass
+                }
+                t = t_next;
             }
             tc::mma_commit(&a_empty[s]);
         }
         if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
+        if (b1_uses > 0) pt_wait(b1_free, (b1_uses - 1) & 1u, &s_abort, err);
+        if (pending) pt_wait(&b_full[1], (b1_loads - 1) & 1u, &s_abort, err);
     }
     tc::fence_before_sync();
     __syncthreads();
