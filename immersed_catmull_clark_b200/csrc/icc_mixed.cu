@@ -273,36 +273,31 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             const int b = blockIdx.x + it * gridDim.x;
             const RowMeta cur = next;
             if (it + 1 < nmine) next = row_meta(g, b + gridDim.x, r, type_id, scale, pass_start, pass_type);
-            float res[81];
-#pragma unroll
-            for (int n = 0; n < 81; ++n) res[n] = 0.f;
+            const int y = it & 1;
+            if (it >= 2) pt_wait(&y_empty[y], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
+            float *sYr = sYb + y * kYFl + r * 81;
             int t = cur.t0;
             for (int pi = cur.p0; pi < cur.p1; ++pi, ++j) {
                 const int t_next = pi + 1 < cur.p1 ? pass_type[pi + 1] : -1;
                 pt_wait(d_full, uint32_t(j) & 1u, &s_abort, err);
                 tc::fence_after_sync();
-                const bool take = cur.type == t;
-#pragma unroll
-                for (int cc = 0; cc < kTcN / 16; ++cc) {
-                    uint32_t rr[16];
-                    tc::tmem_ld16(dcol + cc * 16, rr);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) {
-                        const int n = cc * 16 + q;
-                        if (n < 81) res[n] = take ? cur.scale * __uint_as_float(rr[q]) : res[n];
-                    }
-                }
+                uint32_t v0[32], v1[32], v2[32];
+                tc::tmem_ld32(dcol, v0);
+                tc::tmem_ld32(dcol + 32, v1);
+                tc::tmem_ld32(dcol + 64, v2);
+                tc::tmem_wait_ld();
                 tc::fence_before_sync();
-                tc::mbar_arrive(d_empty);
-                t = t_next;
-            }
-            const int y = it & 1;
-            if (it >= 2) pt_wait(&y_empty[y], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
-            if (cur.type >= 0) {
-                float *sY = sYb + y * kYFl;
+                tc::mbar_arrive(d_empty);   // the accumulator is free for the next pass
+                if (cur.type == t) {
+                    const float se = cur.scale;
 #pragma unroll
-                for (int n = 0; n < 81; ++n) sY[r * 81 + n] = res[n];
+                    for (int n = 0; n < 32; ++n) sYr[n] = se * __uint_as_float(v0[n]);
+#pragma unroll
+                    for (int n = 0; n < 32; ++n) sYr[32 + n] = se * __uint_as_float(v1[n]);
+#pragma unroll
+                    for (int n = 0; n < 81 - 64; ++n) sYr[64 + n] = se * __uint_as_float(v2[n]);
+                }
+                t = t_next;
             }
             tc::mbar_arrive(&y_full[y]);
         }
