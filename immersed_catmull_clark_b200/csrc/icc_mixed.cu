@@ -192,19 +192,30 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         const int m = tid;
         const int lx = m % kBX, ly = (m / kBX) % kBY, lz = m / (kBX * kBY);
         const int base = (lz * kPY + ly) * kPX + lx;
-        // patch rows (c, pz, py) of kPX floats; thread m < 108 copies row m
+        // patch rows (c, pz, py) of kPX floats; thread m < 108 copies row m and, when the input
+        // is masked, fetches the row's mask bytes alongside (applied once the row has landed)
+        uint32_t mbits_next = 0x3FFu;
         auto load_patch = [&](int b, float *dst) {
+            mbits_next = 0x3FFu;
             if (m < 3 * kPZ * kPY) {
                 const BrickBox bb = brick_box(g, b);
                 const int c = m / (kPZ * kPY), py = m % kPY, pz = (m / kPY) % kPZ;
                 const int gy = bb.y0 + py, gz = bb.z0 + pz;
                 float *drow = dst + m * kPX;
                 if (gy < g.cy && gz < g.cz) {
-                    const float *srow = x + (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
+                    const long long off = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
+                    const float *srow = x + off;
 #pragma unroll
                     for (int px = 0; px < kPX; ++px) {
                         if (bb.x0 + px < g.cx) tc::cp_async4(drow + px, srow + px);
                         else drow[px] = 0.f;
+                    }
+                    if (mask_in) {
+                        uint32_t bits = 0;
+#pragma unroll
+                        for (int px = 0; px < kPX; ++px)
+                            if (bb.x0 + px < g.cx && mask[off + px]) bits |= 1u << px;
+                        mbits_next = bits;
                     }
                 } else {
 #pragma unroll
@@ -218,19 +229,16 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             const int b = blockIdx.x + it * gridDim.x;
             const int s = it & 1;
             float *P = sP + s * 3 * kPVol;
+            const uint32_t mbits = mbits_next;   // mask of this thread's row of brick it
             if (it + 1 < nmine) load_patch(b + gridDim.x, sP + ((it + 1) & 1) * 3 * kPVol);
             else tc::cp_async_commit();
             tc::cp_async_wait<1>();
             const BrickBox bb = brick_box(g, b);
-            if (mask_in) {
-                for (int i = m; i < 3 * kPVol; i += 128) {
-                    int c = i / kPVol, r = i - c * kPVol;
-                    int px = r % kPX, py = (r / kPX) % kPY, pz = r / (kPX * kPY);
-                    int gx = bb.x0 + px, gy = bb.y0 + py, gz = bb.z0 + pz;
-                    if (gx < g.cx && gy < g.cy && gz < g.cz &&
-                        !mask[(long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + gx])
-                        P[i] = 0.f;
-                }
+            if (mask_in && m < 3 * kPZ * kPY && mbits != 0x3FFu) {
+                float *row = P + m * kPX;   // this thread's own cp.async row: visible after the wait
+#pragma unroll
+                for (int px = 0; px < kPX; ++px)
+                    if (!(mbits >> px & 1u)) row[px] = 0.f;
             }
             tc::named_sync(1, 128);
             if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
@@ -313,27 +321,43 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             pt_wait(&y_full[y], uint32_t(it >> 1) & 1u, &s_abort, err);
             const float *sY = sYb + y * kYFl;
             if (active) {
-                // a warp task is 3 patch rows; lane = (row, px) sums the <= 27 element contributions
-                // of one node; lanes along x hit distinct banks (element stride 81)
+                // this warp's 9 tasks of 3 patch rows each (rows (q4 + 4 t) * 3 + lrow) run
+                // interleaved: lane = (row, px) sums the <= 27 element contributions of one node
+                // per task, with 9 independent accumulators; lanes along x hit distinct banks
                 const bool okx[3] = {px < bb.ex_n, px >= 1 && px - 1 < bb.ex_n, px >= 2 && px - 2 < bb.ex_n};
-                for (int task = q4; task < kPZ * kPY; task += 4) {
-                    const int row = task * 3 + lrow;   // 0 .. 107 = (c, pz, py)
+                int yoff[9];
+                unsigned okyz[9];
+                float acc[9];
+#pragma unroll
+                for (int t = 0; t < 9; ++t) {
+                    const int row = (q4 + 4 * t) * 3 + lrow;   // (c, pz, py)
                     const int c = row / (kPZ * kPY), py = row % kPY, pz = (row / kPY) % kPZ;
-                    const bool oky[3] = {py < bb.ey_n, py >= 1 && py - 1 < bb.ey_n, py >= 2 && py - 2 < bb.ey_n};
-                    const bool okz[3] = {pz < bb.ez_n, pz >= 1 && pz - 1 < bb.ez_n, pz >= 2 && pz - 2 < bb.ez_n};
-                    // element (px-dx, py-dy, pz-dz), local DOF c*27 + dx + 3 dy + 9 dz
-                    const float *Yb = sY + (px + kBX * (py + kBY * pz)) * 81 + c * 27;
-                    float sum = 0.f;
+                    yoff[t] = (px + kBX * (py + kBY * pz)) * 81 + c * 27;
+                    unsigned m = 0;
 #pragma unroll
-                    for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-                        for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-                            for (int dx = 0; dx < 3; ++dx)
-                                if (okz[dz] && oky[dy] && okx[dx])
-                                    sum += Yb[-(dx + kBX * (dy + kBY * dz)) * 81 + dx + 3 * dy + 9 * dz];
-                    patch_out[(size_t)b * 3 * kPVol + row * kPX + px] = sum;
+                    for (int d = 0; d < 3; ++d) {
+                        if (py >= d && py - d < bb.ey_n) m |= 1u << d;
+                        if (pz >= d && pz - d < bb.ez_n) m |= 8u << d;
+                    }
+                    okyz[t] = m;
+                    acc[t] = 0.f;
                 }
+#pragma unroll
+                for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                        for (int dx = 0; dx < 3; ++dx) {
+                            // element (px-dx, py-dy, pz-dz), local DOF c*27 + dx + 3 dy + 9 dz
+                            const int off = -(dx + kBX * (dy + kBY * dz)) * 81 + dx + 3 * dy + 9 * dz;
+                            const unsigned need = (1u << dy) | (8u << dz);
+#pragma unroll
+                            for (int t = 0; t < 9; ++t)
+                                if (okx[dx] && (okyz[t] & need) == need) acc[t] += sY[yoff[t] + off];
+                        }
+                float *ob = patch_out + (size_t)b * 3 * kPVol + px;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) ob[((q4 + 4 * t) * 3 + lrow) * kPX] = acc[t];
             }
             tc::mbar_arrive(&y_empty[y]);
         }
