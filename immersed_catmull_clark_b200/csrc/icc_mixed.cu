@@ -70,26 +70,25 @@ struct MixedState {
 // ------------------------------------------------------------------------------------------
 
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
-// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (13 warps):
+// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (9 warps):
 //   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; split the current
 //     brick's gathered element vectors into TF32 hi/lo and store them as the A operand straight
 //     into TMEM (row m = element m = lane m), double-buffered in two A slots;
-//   warp 12 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
+//   warp 8 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
 //     element type, buffer 1 for the others, fetched with cp.async.bulk and prefetched while a
 //     main-type pass runs), issues the 33 tcgen05.mma (A from TMEM, B from shared memory) per
 //     type pass into one TMEM accumulator;
-//   warps 4-7 (drain): read the accumulator with tcgen05.ld, keep each row's own type pass, scale
-//     by s_e and stage the brick's element results in shared memory (two staging buffers);
-//   warps 8-11 (sum): add up the staged results per patch node and write the brick partials.
-// mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), y_full/y_empty (staging
-// buffers), b_full/b1_free (B buffers).  Every wait is bounded; on time-out the CTA raises a shared
+//   warps 4-7 (epilogue): read the accumulator with tcgen05.ld, keep each row's own type pass,
+//     scale by s_e and sum the element results per patch node with warp shuffles (x, y) and a
+//     small shared buffer (z), then write the brick partials.
+// mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), b_full/b1_free (B buffers).  Every wait is bounded; on time-out the CTA raises a shared
 // abort flag, so all roles finish promptly and the host reports ICC_TIMEOUT.
-constexpr int kPtThreads = 13 * 32;
+constexpr int kPtThreads = 9 * 32;
 constexpr int kColSlot = 176;    // A slot s: hi at s*176 + [0,88), lo at s*176 + 88 + [0,88)
 constexpr int kColD = 352;       // accumulator: 96 columns
 constexpr uint32_t kPtTmemCols = 512;
-constexpr int kYFl = kEPB * 81;  // one staging buffer
-constexpr int kPtSmem = (4 * kBFl + 2 * 3 * kPVol + 2 * kYFl) * 4;  // 226,752 B
+constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
+constexpr int kPtSmem = (4 * kBFl + 2 * 3 * kPVol + 2 * kZFl) * 4;  // 161,280 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // one type, hi + lo
 
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
@@ -152,12 +151,12 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [2 buffers][hi, lo][kBFl]
     float *sP = psm + 4 * kBFl;           // [2][3 * kPVol]
-    float *sYb = sP + 2 * 3 * kPVol;      // [2][kEPB][81]
-    __shared__ __align__(8) uint64_t bars[13];
+    float *sZb = sP + 2 * 3 * kPVol;      // [2][kZFl] per-layer node partials
+    __shared__ __align__(8) uint64_t bars[9];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *y_full = bars + 6,
-             *y_empty = bars + 8, *b_full = bars + 10, *b1_free = bars + 12;
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *b_full = bars + 6,
+             *b1_free = bars + 8;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
@@ -171,10 +170,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         tc::mbar_init(&a_empty[1], 1);
         tc::mbar_init(d_full, 1);
         tc::mbar_init(d_empty, 128);
-        tc::mbar_init(&y_full[0], 128);
-        tc::mbar_init(&y_full[1], 128);
-        tc::mbar_init(&y_empty[0], 128);
-        tc::mbar_init(&y_empty[1], 128);
         tc::mbar_init(&b_full[0], 1);
         tc::mbar_init(&b_full[1], 1);
         tc::mbar_init(b1_free, 1);
@@ -270,10 +265,15 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         }
         tc::cp_async_wait<0>();
     } else if (warp < 8) {
-        // ------------------------------ drain ------------------------------
+        // ------------------------------ epilogue ------------------------------
+        // Warp q4 holds z-layer lz = q4 of the brick: lane = lx + 8 ly = element (lx, ly, q4) and
+        // TMEM lane 32 q4 + lane.  Node sums run in registers: along x with shuffles by 1 and 2
+        // lanes, along y by 8 and 16 lanes, and the 4 layers are combined through shared memory.
         const int q4 = warp & 3;
-        const int r = q4 * 32 + lane;   // TMEM lane quadrant of this warp = its rows
+        const int r = q4 * 32 + lane;
+        const int lx = lane & 7, ly = lane >> 3;
         const uint32_t dcol = tmem + ((uint32_t)(q4 * 32) << 16) + kColD;
+        const unsigned FULL = 0xffffffffu;
         int j = 0;
         RowMeta next{};
         if (nmine > 0) next = row_meta(g, blockIdx.x, r, type_id, scale, pass_start, pass_type);
@@ -281,9 +281,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             const int b = blockIdx.x + it * gridDim.x;
             const RowMeta cur = next;
             if (it + 1 < nmine) next = row_meta(g, b + gridDim.x, r, type_id, scale, pass_start, pass_type);
-            const int y = it & 1;
-            if (it >= 2) pt_wait(&y_empty[y], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
-            float *sYr = sYb + y * kYFl + r * 81;
+            float res[81];
+#pragma unroll
+            for (int n = 0; n < 81; ++n) res[n] = 0.f;
             int t = cur.t0;
             for (int pi = cur.p0; pi < cur.p1; ++pi, ++j) {
                 const int t_next = pi + 1 < cur.p1 ? pass_type[pi + 1] : -1;
@@ -296,70 +296,73 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                 tc::tmem_wait_ld();
                 tc::fence_before_sync();
                 tc::mbar_arrive(d_empty);   // the accumulator is free for the next pass
-                if (cur.type == t) {
-                    const float se = cur.scale;
+                const bool take = cur.type == t;
+                const float se = cur.scale;
 #pragma unroll
-                    for (int n = 0; n < 32; ++n) sYr[n] = se * __uint_as_float(v0[n]);
+                for (int n = 0; n < 32; ++n) res[n] = take ? se * __uint_as_float(v0[n]) : res[n];
 #pragma unroll
-                    for (int n = 0; n < 32; ++n) sYr[32 + n] = se * __uint_as_float(v1[n]);
+                for (int n = 0; n < 32; ++n) res[32 + n] = take ? se * __uint_as_float(v1[n]) : res[32 + n];
 #pragma unroll
-                    for (int n = 0; n < 81 - 64; ++n) sYr[64 + n] = se * __uint_as_float(v2[n]);
-                }
+                for (int n = 0; n < 17; ++n) res[64 + n] = take ? se * __uint_as_float(v2[n]) : res[64 + n];
                 t = t_next;
             }
-            tc::mbar_arrive(&y_full[y]);
-        }
-    } else if (warp < 12) {
-        // ------------------------------ sum ------------------------------
-        const int q4 = warp & 3;
-        const bool active = lane < 3 * kPX;
-        const int lrow = lane / kPX, px = lane % kPX;
-        for (int it = 0; it < nmine; ++it) {
-            const int b = blockIdx.x + it * gridDim.x;
-            const int y = it & 1;
-            const BrickBox bb = brick_box(g, b);
-            pt_wait(&y_full[y], uint32_t(it >> 1) & 1u, &s_abort, err);
-            const float *sY = sYb + y * kYFl;
-            if (active) {
-                // this warp's 9 tasks of 3 patch rows each (rows (q4 + 4 t) * 3 + lrow) run
-                // interleaved: lane = (row, px) sums the <= 27 element contributions of one node
-                // per task, with 9 independent accumulators; lanes along x hit distinct banks
-                const bool okx[3] = {px < bb.ex_n, px >= 1 && px - 1 < bb.ex_n, px >= 2 && px - 2 < bb.ex_n};
-                int yoff[9];
-                unsigned okyz[9];
-                float acc[9];
+            // x: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2); lanes lx = 7 also carry
+            // px = 8 (v[1](7) + v[2](6)) and px = 9 (v[2](7)).  q = c*9 + az*3 + ay.
+            float X[27], X8[27], X9[27];
 #pragma unroll
-                for (int t = 0; t < 9; ++t) {
-                    const int row = (q4 + 4 * t) * 3 + lrow;   // (c, pz, py)
-                    const int c = row / (kPZ * kPY), py = row % kPY, pz = (row / kPY) % kPZ;
-                    yoff[t] = (px + kBX * (py + kBY * pz)) * 81 + c * 27;
-                    unsigned m = 0;
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        if (py >= d && py - d < bb.ey_n) m |= 1u << d;
-                        if (pz >= d && pz - d < bb.ez_n) m |= 8u << d;
+                for (int az = 0; az < 3; ++az)
+#pragma unroll
+                    for (int ay = 0; ay < 3; ++ay) {
+                        const int q = c * 9 + az * 3 + ay, o = c * 27 + 3 * ay + 9 * az;
+                        const float a0 = res[o], a1 = res[o + 1], a2 = res[o + 2];
+                        const float u1 = __shfl_up_sync(FULL, a1, 1), u2 = __shfl_up_sync(FULL, a2, 2);
+                        const float w1 = __shfl_up_sync(FULL, a2, 1);
+                        X[q] = (a0 + (lx >= 1 ? u1 : 0.f)) + (lx >= 2 ? u2 : 0.f);
+                        X8[q] = a1 + (lx >= 1 ? w1 : 0.f);
+                        X9[q] = a2;
                     }
-                    okyz[t] = m;
-                    acc[t] = 0.f;
-                }
+            // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also carry
+            // py = 4 and py = 5.  Results go to this layer's partials for z-offset az.
+            float *sZ = sZb + (it & 1) * kZFl;
 #pragma unroll
-                for (int dz = 0; dz < 3; ++dz)
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                    for (int dy = 0; dy < 3; ++dy)
+                for (int az = 0; az < 3; ++az)
 #pragma unroll
-                        for (int dx = 0; dx < 3; ++dx) {
-                            // element (px-dx, py-dy, pz-dz), local DOF c*27 + dx + 3 dy + 9 dz
-                            const int off = -(dx + kBX * (dy + kBY * dz)) * 81 + dx + 3 * dy + 9 * dz;
-                            const unsigned need = (1u << dy) | (8u << dz);
-#pragma unroll
-                            for (int t = 0; t < 9; ++t)
-                                if (okx[dx] && (okyz[t] & need) == need) acc[t] += sY[yoff[t] + off];
+                    for (int var = 0; var < 3; ++var) {
+                        const float *V = var == 0 ? X : (var == 1 ? X8 : X9);
+                        const int q = c * 9 + az * 3;
+                        const float a0 = V[q], a1 = V[q + 1], a2 = V[q + 2];
+                        const float s1 = __shfl_up_sync(FULL, a1, 8), s2 = __shfl_up_sync(FULL, a2, 16);
+                        const float t1 = __shfl_up_sync(FULL, a2, 8);
+                        const float yv = (a0 + (ly >= 1 ? s1 : 0.f)) + (ly >= 2 ? s2 : 0.f);
+                        const float y4 = a1 + (ly >= 1 ? t1 : 0.f);
+                        const float y5 = a2;
+                        const int px = var == 0 ? lx : 7 + var;
+                        if (var == 0 || lx == 7) {
+                            float *zb = sZ + (((q4 * 3 + az) * 3 + c) * kPY) * kPX + px;
+                            zb[ly * kPX] = yv;
+                            if (ly == 3) {
+                                zb[4 * kPX] = y4;
+                                zb[5 * kPX] = y5;
+                            }
                         }
-                float *ob = patch_out + (size_t)b * 3 * kPVol + px;
+                    }
+            tc::named_sync(2, 128);
+            // z: node pz = lz + az; sum the <= 3 layers in increasing az
+            for (int i = r; i < 3 * kPVol; i += 128) {
+                const int c = i / kPVol, rem = i - c * kPVol;
+                const int px = rem % kPX, py = (rem / kPX) % kPY, pz = rem / (kPX * kPY);
+                float sum = 0.f;
 #pragma unroll
-                for (int t = 0; t < 9; ++t) ob[((q4 + 4 * t) * 3 + lrow) * kPX] = acc[t];
+                for (int az = 0; az < 3; ++az) {
+                    const int lz = pz - az;
+                    if (lz >= 0 && lz < kBZ) sum += sZ[(((lz * 3 + az) * 3 + c) * kPY + py) * kPX + px];
+                }
+                patch_out[(size_t)b * 3 * kPVol + i] = sum;
             }
-            tc::mbar_arrive(&y_empty[y]);
         }
     } else if (lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
