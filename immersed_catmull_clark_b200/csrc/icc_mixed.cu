@@ -70,20 +70,21 @@ struct MixedState {
 // ------------------------------------------------------------------------------------------
 
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
-// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (9 warps):
+// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (13 warps):
 //   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; split the current
 //     brick's gathered element vectors into TF32 hi/lo and store them as the A operand straight
 //     into TMEM (row m = element m = lane m), double-buffered in two A slots;
-//   warp 8 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
+//   warp 12 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
 //     element type, buffer 1 for the others, fetched with cp.async.bulk and prefetched while a
 //     main-type pass runs), issues the 33 tcgen05.mma (A from TMEM, B from shared memory) per
 //     type pass into one TMEM accumulator;
-//   warps 4-7 (epilogue): read the accumulator with tcgen05.ld, keep each row's own type pass,
-//     scale by s_e and sum the element results per patch node with warp shuffles (x, y) and a
-//     small shared buffer (z), then write the brick partials.
+//   warps 4-11 (epilogue, two groups of 4 taking alternate bricks): read the accumulator with
+//     tcgen05.ld, keep each row's own type pass, scale by s_e and sum the element results per
+//     patch node with warp shuffles (x, y) and a small shared buffer (z), then write the brick
+//     partials.
 // mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), b_full/b1_free (B buffers).  Every wait is bounded; on time-out the CTA raises a shared
 // abort flag, so all roles finish promptly and the host reports ICC_TIMEOUT.
-constexpr int kPtThreads = 9 * 32;
+constexpr int kPtThreads = 13 * 32;
 constexpr int kColSlot = 176;    // A slot s: hi at s*176 + [0,88), lo at s*176 + 88 + [0,88)
 constexpr int kColD = 352;       // accumulator: 96 columns
 constexpr uint32_t kPtTmemCols = 512;
@@ -264,58 +265,63 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             tc::named_sync(1, 128);   // everyone is done with P before the next prefetch reuses it
         }
         tc::cp_async_wait<0>();
-    } else if (warp < 8) {
+    } else if (warp < 12) {
         // ------------------------------ epilogue ------------------------------
-        // Warp q4 holds z-layer lz = q4 of the brick: lane = lx + 8 ly = element (lx, ly, q4) and
+        // Two groups of 4 warps take alternate bricks (group eg = brick parity), so one group can
+        // drain the accumulator for the next brick while the other still sums nodes.  Warp q4 of
+        // a group holds z-layer lz = q4 of its brick: lane = lx + 8 ly = element (lx, ly, q4) and
         // TMEM lane 32 q4 + lane.  Node sums run in registers: along x with shuffles by 1 and 2
-        // lanes, along y by 8 and 16 lanes, and the 4 layers are combined through shared memory.
+        // lanes, along y by 8 and 16 lanes; the 4 layers are combined through shared memory.
+        const int eg = (warp - 4) >> 2;
         const int q4 = warp & 3;
         const int r = q4 * 32 + lane;
         const int lx = lane & 7, ly = lane >> 3;
         const uint32_t dcol = tmem + ((uint32_t)(q4 * 32) << 16) + kColD;
         const unsigned FULL = 0xffffffffu;
-        int j = 0;
-        RowMeta next{};
-        if (nmine > 0) next = row_meta(g, blockIdx.x, r, type_id, scale, pass_start, pass_type);
+        float *sZ = sZb + eg * kZFl;
+        int j = 0;   // global pass index of the brick's first pass
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
-            const RowMeta cur = next;
-            if (it + 1 < nmine) next = row_meta(g, b + gridDim.x, r, type_id, scale, pass_start, pass_type);
+            const int p0 = pass_start[b], p1 = pass_start[b + 1];
+            if ((it & 1) != eg) {
+                j += p1 - p0;
+                continue;
+            }
+            const RowMeta cur = row_meta(g, b, r, type_id, scale, pass_start, pass_type);
             float res[81];
 #pragma unroll
             for (int n = 0; n < 81; ++n) res[n] = 0.f;
             int t = cur.t0;
-            for (int pi = cur.p0; pi < cur.p1; ++pi, ++j) {
-                const int t_next = pi + 1 < cur.p1 ? pass_type[pi + 1] : -1;
+            for (int pi = p0; pi < p1; ++pi, ++j) {
+                const int t_next = pi + 1 < p1 ? pass_type[pi + 1] : -1;
                 pt_wait(d_full, uint32_t(j) & 1u, &s_abort, err);
                 tc::fence_after_sync();
-                uint32_t v0[32], v1[32], v2[32];
-                tc::tmem_ld32(dcol, v0);
-                tc::tmem_ld32(dcol + 32, v1);
-                tc::tmem_ld32(dcol + 64, v2);
-                tc::tmem_wait_ld();
-                tc::fence_before_sync();
-                tc::mbar_arrive(d_empty);   // the accumulator is free for the next pass
                 const bool take = cur.type == t;
                 const float se = cur.scale;
 #pragma unroll
-                for (int n = 0; n < 32; ++n) res[n] = take ? se * __uint_as_float(v0[n]) : res[n];
+                for (int ch = 0; ch < 3; ++ch) {
+                    uint32_t v[32];
+                    tc::tmem_ld32(dcol + ch * 32, v);
+                    tc::tmem_wait_ld();
 #pragma unroll
-                for (int n = 0; n < 32; ++n) res[32 + n] = take ? se * __uint_as_float(v1[n]) : res[32 + n];
-#pragma unroll
-                for (int n = 0; n < 17; ++n) res[64 + n] = take ? se * __uint_as_float(v2[n]) : res[64 + n];
+                    for (int n = 0; n < 32; ++n)
+                        if (ch * 32 + n < 81) res[ch * 32 + n] = take ? se * __uint_as_float(v[n]) : res[ch * 32 + n];
+                }
+                tc::fence_before_sync();
+                tc::mbar_arrive(d_empty);   // the accumulator is free for the next pass
                 t = t_next;
             }
-            // x: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2); lanes lx = 7 also carry
-            // px = 8 (v[1](7) + v[2](6)) and px = 9 (v[2](7)).  q = c*9 + az*3 + ay.
-            float X[27], X8[27], X9[27];
+            tc::named_sync(2 + eg, 128);   // this group's previous z-sum is done with sZ
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+            for (int c = 0; c < 3; ++c) {
+                // x: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2); lanes lx = 7 also
+                // carry px = 8 (v[1](7) + v[2](6)) and px = 9 (v[2](7)).  q = az*3 + ay.
+                float X[9], X8[9], X9[9];
 #pragma unroll
                 for (int az = 0; az < 3; ++az)
 #pragma unroll
                     for (int ay = 0; ay < 3; ++ay) {
-                        const int q = c * 9 + az * 3 + ay, o = c * 27 + 3 * ay + 9 * az;
+                        const int q = az * 3 + ay, o = c * 27 + 3 * ay + 9 * az;
                         const float a0 = res[o], a1 = res[o + 1], a2 = res[o + 2];
                         const float u1 = __shfl_up_sync(FULL, a1, 1), u2 = __shfl_up_sync(FULL, a2, 2);
                         const float w1 = __shfl_up_sync(FULL, a2, 1);
@@ -323,45 +329,43 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                         X8[q] = a1 + (lx >= 1 ? w1 : 0.f);
                         X9[q] = a2;
                     }
-            // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also carry
-            // py = 4 and py = 5.  Results go to this layer's partials for z-offset az.
-            float *sZ = sZb + (it & 1) * kZFl;
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
+                // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also
+                // carry py = 4 and py = 5.  Results are this layer's partials for z-offset az.
 #pragma unroll
                 for (int az = 0; az < 3; ++az)
 #pragma unroll
                     for (int var = 0; var < 3; ++var) {
                         const float *V = var == 0 ? X : (var == 1 ? X8 : X9);
-                        const int q = c * 9 + az * 3;
+                        const int q = az * 3;
                         const float a0 = V[q], a1 = V[q + 1], a2 = V[q + 2];
                         const float s1 = __shfl_up_sync(FULL, a1, 8), s2 = __shfl_up_sync(FULL, a2, 16);
                         const float t1 = __shfl_up_sync(FULL, a2, 8);
                         const float yv = (a0 + (ly >= 1 ? s1 : 0.f)) + (ly >= 2 ? s2 : 0.f);
                         const float y4 = a1 + (ly >= 1 ? t1 : 0.f);
-                        const float y5 = a2;
                         const int px = var == 0 ? lx : 7 + var;
                         if (var == 0 || lx == 7) {
                             float *zb = sZ + (((q4 * 3 + az) * 3 + c) * kPY) * kPX + px;
                             zb[ly * kPX] = yv;
                             if (ly == 3) {
                                 zb[4 * kPX] = y4;
-                                zb[5 * kPX] = y5;
+                                zb[5 * kPX] = a2;
                             }
                         }
                     }
-            tc::named_sync(2, 128);
+            }
+            tc::named_sync(2 + eg, 128);
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
+            float *ob = patch_out + (size_t)b * 3 * kPVol;
             for (int i = r; i < 3 * kPVol; i += 128) {
                 const int c = i / kPVol, rem = i - c * kPVol;
-                const int px = rem % kPX, py = (rem / kPX) % kPY, pz = rem / (kPX * kPY);
+                const int pz = rem / (kPX * kPY), pyx = rem - pz * (kPX * kPY);
                 float sum = 0.f;
 #pragma unroll
                 for (int az = 0; az < 3; ++az) {
                     const int lz = pz - az;
-                    if (lz >= 0 && lz < kBZ) sum += sZ[(((lz * 3 + az) * 3 + c) * kPY + py) * kPX + px];
+                    if (lz >= 0 && lz < kBZ) sum += sZ[((lz * 3 + az) * 3 + c) * (kPY * kPX) + pyx];
                 }
-                patch_out[(size_t)b * 3 * kPVol + i] = sum;
+                ob[i] = sum;
             }
         }
     } else if (lane == 0) {
