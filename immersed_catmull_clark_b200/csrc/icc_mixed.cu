@@ -82,8 +82,9 @@ struct MixedState {
 //     tcgen05.ld, keep each row's own type pass, scale by s_e and sum the element results per
 //     patch node with warp shuffles (x, y) and a small shared buffer (z), then write the brick
 //     partials.
-// mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), b_full/b1_free (B buffers).  Every wait is bounded; on time-out the CTA raises a shared
-// abort flag, so all roles finish promptly and the host reports ICC_TIMEOUT.
+// mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), b_full/b1_free (B buffers).
+// Every wait is bounded; on time-out the CTA raises a shared abort flag, so all roles finish
+// promptly and the host reports ICC_TIMEOUT.
 constexpr int kPtThreads = 13 * 32;
 constexpr int kColSlot = 176;    // A slot s: hi at s*176 + [0,88), lo at s*176 + 88 + [0,88)
 constexpr int kColD = 352;       // accumulator: 96 columns
@@ -153,11 +154,13 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
     float *sB = psm;                      // [2 buffers][hi, lo][kBFl]
     float *sP = psm + 4 * kBFl;           // [2][3 * kPVol]
     float *sZb = sP + 2 * 3 * kPVol;      // [2][kZFl] per-layer node partials
-    __shared__ __align__(8) uint64_t bars[9];
+    __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *b_full = bars + 6,
-             *b1_free = bars + 8;
+    // d_full has one barrier per epilogue group: a group waits only for its own bricks' passes, so
+    // its parity waits never run two phases ahead of the barrier
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 7,
+             *b1_free = bars + 9;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
@@ -169,7 +172,8 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         tc::mbar_init(&a_full[1], 128);
         tc::mbar_init(&a_empty[0], 1);
         tc::mbar_init(&a_empty[1], 1);
-        tc::mbar_init(d_full, 1);
+        tc::mbar_init(&d_full[0], 1);
+        tc::mbar_init(&d_full[1], 1);
         tc::mbar_init(d_empty, 128);
         tc::mbar_init(&b_full[0], 1);
         tc::mbar_init(&b_full[1], 1);
@@ -279,14 +283,11 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         const uint32_t dcol = tmem + ((uint32_t)(q4 * 32) << 16) + kColD;
         const unsigned FULL = 0xffffffffu;
         float *sZ = sZb + eg * kZFl;
-        int j = 0;   // global pass index of the brick's first pass
+        int j = 0;   // passes of this group's bricks so far (phases of d_full[eg])
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
             const int p0 = pass_start[b], p1 = pass_start[b + 1];
-            if ((it & 1) != eg) {
-                j += p1 - p0;
-                continue;
-            }
+            if ((it & 1) != eg) continue;
             const RowMeta cur = row_meta(g, b, r, type_id, scale, pass_start, pass_type);
             float res[81];
 #pragma unroll
@@ -294,7 +295,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             int t = cur.t0;
             for (int pi = p0; pi < p1; ++pi, ++j) {
                 const int t_next = pi + 1 < p1 ? pass_type[pi + 1] : -1;
-                pt_wait(d_full, uint32_t(j) & 1u, &s_abort, err);
+                pt_wait(&d_full[eg], uint32_t(j) & 1u, &s_abort, err);
                 tc::fence_after_sync();
                 const bool take = cur.type == t;
                 const float se = cur.scale;
@@ -419,7 +420,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                     tc::mma_tf32_ts(tmem + kColD, ah, dbl, idesc, 1u);
                     tc::mma_tf32_ts(tmem + kColD, ah, dbh, idesc, 1u);
                 }
-                tc::mma_commit(d_full);
+                tc::mma_commit(&d_full[it & 1]);
                 if (buf == 1) {
                     tc::mma_commit(b1_free);
                     b1_uses++;

@@ -37,6 +37,21 @@ def test_tc_apply_matches_oracle(nsub):
     assert rel(y, k.matvec(x.astype(np.float64))) < TC_APPLY_TOL
 
 
+@pytest.mark.parametrize("nsub,masked", [([64, 32, 24], False), ([72, 30, 26], True), ([128, 64, 64], True)])
+def test_tc_apply_many_bricks_per_cta(nsub, masked):
+    # more bricks than SMs: every persistent CTA walks several bricks (A-slot, accumulator and
+    # staging reuse across bricks), checked against the oracle's matrix-free element loop
+    sp, osp, em, s, rng = setup(nsub, seed=8)
+    fm = (rng.uniform(size=sp.ndof) > 0.1).astype(np.uint8) if masked else None
+    mode = icc.MASK_ZERO if masked else icc.MASK_NONE
+    op = icc.MatrixFreeOperator(sp, em, s, fm, mode)
+    x = rng.standard_normal(sp.ndof).astype(np.float32)
+    y = op.matvec_f32(x)
+    yo = O.mf_apply(osp, em.types, em.type_id.astype(np.int64), s, x.astype(np.float64), fm, mode)
+    assert rel(y, yo) < TC_APPLY_TOL
+    assert np.array_equal(y, op.matvec_f32(x))
+
+
 def test_tc_apply_masked_and_deterministic():
     sp, osp, em, s, rng = setup([9, 5, 6], seed=4)
     fm = (rng.uniform(size=sp.ndof) > 0.25).astype(np.uint8)
