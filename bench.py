@@ -355,7 +355,9 @@ def run_ours(args):
                "gpu_launches": int(launches),
                "clocks": clk.summary(),
                "accuracy": err,
-               "solve_info": {"rel_res": info.rel_res, "device_ms": info.device_ms}}
+               "solve_info": {"rel_res": info.rel_res, "device_ms": info.device_ms,
+                              "iterations": int(info.iterations), "residual_replacements": int(info.outer_iterations),
+                              "fp64_applies": int(info.fp64_applies), "tc_applies": int(info.mixed_applies)}}
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()

@@ -55,7 +55,7 @@ struct MixedState {
     int *d_pass_start = nullptr, *d_pass_type = nullptr;
     float *d_patch32 = nullptr;
     float *d_rhs32 = nullptr, *d_x32 = nullptr, *d_r32 = nullptr, *d_p32 = nullptr, *d_ap32 = nullptr,
-          *d_inv32 = nullptr;
+          *d_inv32 = nullptr, *d_xm32 = nullptr;   // xm32: masked input of the brick apply
     double *d_x64 = nullptr, *d_r64 = nullptr, *d_y64 = nullptr, *d_scalars = nullptr;
     int *d_err = nullptr;
     int main_type = 0;               // most frequent pass type: pinned in B buffer 0
@@ -145,8 +145,7 @@ __device__ __forceinline__ RowMeta row_meta(const Geom &g, int b, int r, const i
 }
 
 __global__ void __launch_bounds__(kPtThreads, 1)
-apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__ mask, int mask_in,
-                const float *__restrict__ scale, const int *__restrict__ type_id, const float4 *__restrict__ bmat,
+apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ scale, const int *__restrict__ type_id, const float4 *__restrict__ bmat,
                 int main_type, const int *__restrict__ pass_start, const int *__restrict__ pass_type,
                 float *__restrict__ patch_out, int *__restrict__ err, const PcgState *__restrict__ st) {
     if (st && st->status != 0) return;
@@ -192,11 +191,10 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         const int m = tid;
         const int lx = m % kBX, ly = (m / kBX) % kBY, lz = m / (kBX * kBY);
         const int base = (lz * kPY + ly) * kPX + lx;
-        // patch rows (c, pz, py) of kPX floats; thread m < 108 copies row m and, when the input
-        // is masked, fetches the row's mask bytes alongside (applied once the row has landed)
-        uint32_t mbits_next = 0x3FFu;
+        // patch rows (c, pz, py) of kPX floats; thread m < 108 copies row m, in 8-byte pieces
+        // when the row is whole and starts on an even float (always when the x control-point
+        // count is even), else float by float
         auto load_patch = [&](int b, float *dst) {
-            mbits_next = 0x3FFu;
             if (m < 3 * kPZ * kPY) {
                 const BrickBox bb = brick_box(g, b);
                 const int c = m / (kPZ * kPY), py = m % kPY, pz = (m / kPY) % kPZ;
@@ -205,17 +203,15 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                 if (gy < g.cy && gz < g.cz) {
                     const long long off = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
                     const float *srow = x + off;
+                    if (bb.x0 + kPX <= g.cx && !(off & 1)) {
 #pragma unroll
-                    for (int px = 0; px < kPX; ++px) {
-                        if (bb.x0 + px < g.cx) tc::cp_async4(drow + px, srow + px);
-                        else drow[px] = 0.f;
-                    }
-                    if (mask_in) {
-                        uint32_t bits = 0;
+                        for (int px = 0; px < kPX; px += 2) tc::cp_async8(drow + px, srow + px);
+                    } else {
 #pragma unroll
-                        for (int px = 0; px < kPX; ++px)
-                            if (bb.x0 + px < g.cx && mask[off + px]) bits |= 1u << px;
-                        mbits_next = bits;
+                        for (int px = 0; px < kPX; ++px) {
+                            if (bb.x0 + px < g.cx) tc::cp_async4(drow + px, srow + px);
+                            else drow[px] = 0.f;
+                        }
                     }
                 } else {
 #pragma unroll
@@ -229,23 +225,24 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
             const int b = blockIdx.x + it * gridDim.x;
             const int s = it & 1;
             float *P = sP + s * 3 * kPVol;
-            const uint32_t mbits = mbits_next;   // mask of this thread's row of brick it
             if (it + 1 < nmine) load_patch(b + gridDim.x, sP + ((it + 1) & 1) * 3 * kPVol);
             else tc::cp_async_commit();
             tc::cp_async_wait<1>();
             const BrickBox bb = brick_box(g, b);
-            if (mask_in && m < 3 * kPZ * kPY && mbits != 0x3FFu) {
-                float *row = P + m * kPX;   // this thread's own cp.async row: visible after the wait
-#pragma unroll
-                for (int px = 0; px < kPX; ++px)
-                    if (!(mbits >> px & 1u)) row[px] = 0.f;
-            }
             tc::named_sync(1, 128);
             if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n;
             const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kColSlot);
             const float *Pm = P + base;
+            // Element-local shift: every K_e maps a constant per-component field to zero, so
+            // K_e (u_e - u_c 1_c) = K_e u_e with u_c the element's centre control value of
+            // component c.  The split operands then carry only the variation across the element,
+            // so the TF32 splitting error scales with that variation instead of with |u|, which
+            // matters for the smooth, low-energy vectors of a converging PCG.
+            float ctr[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ctr[c] = valid ? Pm[c * kPVol + kPY * kPX + kPX + 1] : 0.f;
 #pragma unroll
             for (int c8 = 0; c8 < kTcK / 8; ++c8) {
                 float hi[8], lo[8];
@@ -255,10 +252,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                     float v = 0.f;
                     if (k < 81) {
                         const int c = k / 27, a = k % 27;
-                        if (valid) v = Pm[c * kPVol + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
+                        if (valid) v = Pm[c * kPVol + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3] - ctr[c];
                     }
-                    hi[q] = tc::to_tf32(v);
-                    lo[q] = tc::to_tf32(v - hi[q]);
+                    tc::split_tf32(v, hi[q], lo[q]);
                 }
                 tc::tmem_st8(trow + c8 * 8, hi);
                 tc::tmem_st8(trow + kTcK + c8 * 8, lo);
@@ -375,6 +371,11 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
         tc::mbar_arrive_expect_tx(&b_full[0], kBBytes);
         tc::bulk_g2s(sB, bmat + (size_t)main_type * (2 * kBFl / 4), kBBytes, &b_full[0]);
         pt_wait(&b_full[0], 0u, &s_abort, err);
+        // descriptors of K step 0 for both B buffers (hi and lo terms); the shared-memory window
+        // is below 256 KB, so adding a step's offset never carries out of the address field
+        const uint64_t dbh0_base = tc::make_desc(sB, kBLbo, kSbo), dbl0_base = tc::make_desc(sB + kBFl, kBLbo, kSbo);
+        const uint64_t dbh1_base = tc::make_desc(sB + 2 * kBFl, kBLbo, kSbo),
+                       dbl1_base = tc::make_desc(sB + 3 * kBFl, kBLbo, kSbo);
         int tag1 = -1;             // type held (or being fetched) in B buffer 1
         bool pending = false;      // a fetch into buffer 1 has not been waited for yet
         uint32_t b1_loads = 0, b1_uses = 0;
@@ -409,12 +410,13 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const uint8_t *__restrict__
                     }
                 }
                 tc::fence_after_sync();
-                const float *bh0 = sB + buf * 2 * kBFl;
+                const uint64_t dbh0 = buf ? dbh1_base : dbh0_base, dbl0 = buf ? dbl1_base : dbl0_base;
                 const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
-#pragma unroll 1
+#pragma unroll
                 for (int ks = 0; ks < kTcKSteps; ++ks) {
-                    const float *bh = bh0 + ks * 2 * (kTcN / 8) * 32;
-                    const uint64_t dbh = tc::make_desc(bh, kBLbo, kSbo), dbl = tc::make_desc(bh + kBFl, kBLbo, kSbo);
+                    // one K step of 8 = two core-matrix columns: advance the start address field
+                    const uint64_t dk = (uint64_t)(ks * 2 * kBLbo) >> 4;
+                    const uint64_t dbh = dbh0 + dk, dbl = dbl0 + dk;
                     const uint32_t ah = acol + ks * 8, al = acol + kTcK + ks * 8;
                     tc::mma_tf32_ts(tmem + kColD, al, dbh, idesc, ks > 0 ? 1u : 0u);
                     tc::mma_tf32_ts(tmem + kColD, ah, dbl, idesc, 1u);
@@ -580,7 +582,7 @@ static int mixed_init(Op &op) {
     const size_t n = (size_t)op.ndof;
     if ((rc = dalloc(&ms.d_scale32, (size_t)op.nel, "alloc mixed"))) return rc;
     if ((rc = dalloc(&ms.d_patch32, (size_t)g.nbricks * 3 * kPVol, "alloc mixed"))) return rc;
-    float **f32[] = {&ms.d_rhs32, &ms.d_x32, &ms.d_r32, &ms.d_p32, &ms.d_ap32, &ms.d_inv32};
+    float **f32[] = {&ms.d_rhs32, &ms.d_x32, &ms.d_r32, &ms.d_p32, &ms.d_ap32, &ms.d_inv32, &ms.d_xm32};
     for (float **p : f32)
         if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
     double **f64[] = {&ms.d_x64, &ms.d_r64, &ms.d_y64};
@@ -621,30 +623,46 @@ int mixed_on_scale_update(Op &op) {
     return ICC_OK;
 }
 
-// enqueue y32 = A p32 with the tensor-core apply (partials: p'Ap per CTA)
-static void enqueue_apply_tc(Op &op, const float *x, float *y, double *partials, const PcgState *st,
-                             bool input_masked = false) {
+// xm = mask .* x (the brick apply reads its input unmasked)
+__global__ void mask_copy_kernel(long long n, const float *__restrict__ x, const uint8_t *__restrict__ mask,
+                                 float *__restrict__ xm) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        xm[i] = mask[i] ? x[i] : 0.f;
+}
+
+static void launch_apply_tc(Op &op, const float *xin, const PcgState *st) {
     MixedState &ms = *op.mixed;
     const int grid = std::min(op.num_sms, op.g.nbricks);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(
-        op.g, x, op.d_mask, (op.mask_mode != ICC_MASK_NONE && !input_masked) ? 1 : 0, ms.d_scale32, op.d_type_id,
-        ms.d_bmat, ms.main_type, ms.d_pass_start, ms.d_pass_type, ms.d_patch32, ms.d_err, st);
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, op.d_type_id, ms.d_bmat,
+                                                              ms.main_type, ms.d_pass_start, ms.d_pass_type,
+                                                              ms.d_patch32, ms.d_err, st);
+}
+
+// enqueue y32 = A x32 with the tensor-core apply; a masked operator first zeroes the fixed DOFs of
+// the input (into the xm32 scratch vector), the node-side pass applies the output rule
+static void enqueue_apply_tc(Op &op, const float *x, float *y) {
+    MixedState &ms = *op.mixed;
+    const float *xin = x;
+    if (op.mask_mode != ICC_MASK_NONE) {
+        mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.ndof, x, op.d_mask, ms.d_xm32);
+        xin = ms.d_xm32;
+    }
+    launch_apply_tc(op, xin, nullptr);
     gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, x, op.d_mask, op.mask_mode,
-                                                                       y, partials, st);
+                                                                       y, nullptr, nullptr);
 }
 
 // One iteration of the FP32 (sloppy) PCG on the tensor-core operator.  With ICC_MASK_ZERO the
-// search direction is kept zero on fixed DOFs, so the apply needs no input mask.
+// search direction is kept zero on fixed DOFs; with ICC_MASK_IDENTITY the direction update also
+// writes the masked copy the brick apply reads.
 static void enqueue_inner_iteration(Op &op) {
     MixedState &ms = *op.mixed;
     const int vb = op.vec_blocks;
-    const bool pre = op.mask_mode == ICC_MASK_ZERO;
-    const uint8_t *pm = pre ? op.d_mask : nullptr;
-    const int grid = std::min(op.num_sms, op.g.nbricks);
-    pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state, pm);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(
-        op.g, ms.d_p32, op.d_mask, (op.mask_mode != ICC_MASK_NONE && !pre) ? 1 : 0, ms.d_scale32, op.d_type_id,
-        ms.d_bmat, ms.main_type, ms.d_pass_start, ms.d_pass_type, ms.d_patch32, ms.d_err, ms.d_state);
+    const bool zero = op.mask_mode == ICC_MASK_ZERO, ident = op.mask_mode == ICC_MASK_IDENTITY;
+    pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.ndof, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state,
+                                                           zero || ident ? op.d_mask : nullptr,
+                                                           ident ? ms.d_xm32 : nullptr);
+    launch_apply_tc(op, ident ? ms.d_xm32 : ms.d_p32, ms.d_state);
     gather_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, ms.d_p32, op.d_mask, op.mask_mode,
                                                             ms.d_ap32, op.d_partials, ms.d_state, ms.d_state,
                                                             op.d_counter);
@@ -657,7 +675,7 @@ static void enqueue_inner_iteration(Op &op) {
 int mixed_apply_f32(Op &op, const float *x, float *y) {
     int rc = mixed_init(op);
     if (rc) return rc;
-    enqueue_apply_tc(op, x, y, nullptr, nullptr);
+    enqueue_apply_tc(op, x, y);
     ICC_CUDA(cudaGetLastError(), "tc apply launch");
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, op.mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");

@@ -163,6 +163,9 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
 __device__ __forceinline__ void cp_async4(void *dst_smem, const void *src_gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst_smem)), "l"(src_gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src_gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst_smem)), "l"(src_gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -177,6 +180,19 @@ __device__ __forceinline__ float to_tf32(float v) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
     return __uint_as_float(r);
+}
+
+// The same rounding with two integer operations: add half of the dropped 13-bit field to the
+// magnitude and clear the field (finite inputs; a carry into the exponent is the correct result).
+__device__ __forceinline__ float to_tf32_int(float v) {
+    return __uint_as_float((__float_as_uint(v) + 0x1000u) & 0xffffe000u);
+}
+
+// v = hi + lo exactly up to the 13 bits dropped from lo: hi = tf32(v), lo = tf32(v - hi), where
+// v - hi is exact because hi is v rounded to 11 significant bits.
+__device__ __forceinline__ void split_tf32(float v, float &hi, float &lo) {
+    hi = to_tf32_int(v);
+    lo = to_tf32_int(v - hi);
 }
 
 }  // namespace tc

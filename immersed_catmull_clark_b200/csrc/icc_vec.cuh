@@ -191,15 +191,23 @@ pcg_update_kernel(long long n, const T *__restrict__ p, const T *__restrict__ ap
     }
 }
 
-// p = D^-1 r + beta p (rust/src/solver.rs:64-71)
+// p = D^-1 r + beta p (rust/src/solver.rs:64-71).  With pmask: p is kept zero on fixed DOFs, or,
+// when pm is given, p stays whole and pm = pmask .* p is written beside it.
 template <class T>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_p_kernel(long long n, const T *__restrict__ r, const T *__restrict__ inv, T *__restrict__ p,
-             const PcgState *__restrict__ st, const uint8_t *__restrict__ pmask = nullptr) {
+             const PcgState *__restrict__ st, const uint8_t *__restrict__ pmask = nullptr, T *__restrict__ pm = nullptr) {
     if (st->status != 0) return;
     const T beta = T(st->beta);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        p[i] = (pmask && !pmask[i]) ? T(0) : inv[i] * r[i] + beta * p[i];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const T v = inv[i] * r[i] + beta * p[i];
+        if (pm) {
+            p[i] = v;
+            pm[i] = pmask[i] ? v : T(0);
+        } else {
+            p[i] = (pmask && !pmask[i]) ? T(0) : v;
+        }
+    }
 }
 
 }  // namespace icc

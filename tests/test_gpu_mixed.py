@@ -83,3 +83,59 @@ def test_mixed_solve_cantilever():
     xd, itd, resd = icc.PcgSolver(20 * sp.ndof, 1e-12).solve(sp.ndof, b, None, op)
     c_ref, c = p.force @ xd, p.force @ xm
     assert abs(c - c_ref) / abs(c_ref) < 1e-6
+
+
+def test_tc_apply_identity_rows():
+    # ICC_MASK_IDENTITY: K on free rows of the masked input, identity on fixed rows
+    sp, osp, em, s, rng = setup([17, 9, 6], seed=12)
+    fm = (rng.uniform(size=sp.ndof) > 0.2).astype(np.uint8)
+    op = icc.MatrixFreeOperator(sp, em, s, fm, icc.MASK_IDENTITY)
+    x = rng.standard_normal(sp.ndof).astype(np.float32)
+    y = op.matvec_f32(x)
+    yo = O.mf_apply(osp, em.types, em.type_id.astype(np.int64), s, x.astype(np.float64), fm, icc.MASK_IDENTITY)
+    assert rel(y, yo) < TC_APPLY_TOL
+
+
+def test_tc_apply_translation_offset():
+    # K annihilates rigid translations: a large constant added to every component must not
+    # degrade the FP32 result (the split operands carry only each element's variation)
+    sp, osp, em, s, rng = setup([24, 16, 12], seed=13)
+    op = icc.MatrixFreeOperator(sp, em, s)
+    w = rng.standard_normal(sp.ndof)
+    shift = np.repeat([1e3, -2e3, 5e2], sp.ndof_sc)
+    v = (w + shift).astype(np.float32)
+    y = op.matvec_f32(v)
+    yo = O.mf_apply(osp, em.types, em.type_id.astype(np.int64), s, v.astype(np.float64), None, icc.MASK_NONE)
+    assert rel(y, yo) < TC_APPLY_TOL
+
+
+def test_mixed_solve_identity_rows_patch_test():
+    # rust/tests/iga_kernel.rs:94-117 with the mixed-precision solve: identity rows on the
+    # boundary, a linear field recovered to the solver tolerance
+    bounds = ((0.0, 1.0), (0.0, 2.0), (0.5, 1.0))
+    nsub = [10, 8, 6]
+    sp = icc.SpaceBox(bounds, nsub, 2)
+    osp = O.Space(bounds, nsub, 2)
+    lam, mu = icc.lame(1.0, 0.3)
+    em = icc.elasticity_element_matrices(sp, lam, mu)
+    g = osp.greville()
+    nsc = sp.ndof_sc
+    u = np.zeros(sp.ndof)
+    for c in range(3):
+        a = [((c * 3 + j) + 1.0) * 1e-2 - 0.03 for j in range(3)]
+        u[c * nsc:(c + 1) * nsc] = sum(a[j] * g[:, j] for j in range(3)) + 0.1 * (c + 1.0)
+    idx = np.indices(sp.ndof_dir[::-1]).reshape(3, -1)[::-1]
+    on = np.zeros(nsc, dtype=bool)
+    for d in range(3):
+        on |= (idx[d] == 0) | (idx[d] == sp.ndof_dir[d] - 1)
+    fixed = np.tile(on, 3)
+    fm = (~fixed).astype(np.uint8)
+    ub = np.where(fixed, u, 0.0)
+    full = icc.MatrixFreeOperator(sp, em)
+    b = np.where(fixed, ub, -full.matvec(ub))
+    diag = np.where(fixed, 1.0, full.diagonal())
+    op = icc.MatrixFreeOperator(sp, em, None, fm, icc.MASK_IDENTITY)
+    tol = 1e-10
+    x, it, res = icc.PcgSolver(20 * sp.ndof, tol, precision=icc.MIXED).solve(sp.ndof, b, diag, op)
+    assert res < tol
+    assert rel(x, u) < 1e-8
