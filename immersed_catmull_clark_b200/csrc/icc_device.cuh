@@ -74,6 +74,8 @@ struct Op {
     // host copies used by the tensor-core path set-up
     std::vector<double> host_ktypes, host_scale;
     std::vector<int32_t> host_type_id;
+    std::vector<int> host_type1d[3];                     // 1-D type of every element position
+    std::vector<std::array<double, 9>> host_basis1d[3];  // basis values per 1-D type (Space::basis1d)
     MixedState *mixed = nullptr;
 
     ~Op();

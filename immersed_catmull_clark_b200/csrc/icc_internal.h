@@ -22,6 +22,9 @@ struct Space {
     int64_t nel, nsc, ndof;
     std::vector<Mat1d> mats1d[3];  // distinct 1-D matrices per direction
     std::vector<int> type1d[3];    // 1-D type of every element per direction
+    // values of the 3 local basis functions of each 1-D type at 3 points of the element:
+    // basis1d[d][t][3 i + q] = N_i(x_q), x_q at the Gauss points (same relative points for all)
+    std::vector<std::array<double, 9>> basis1d[3];
 
     bool init(const double bounds[6], const int64_t nsub[3]);
     void element_types(double lambda, double mu, std::vector<double> &ke, std::vector<int32_t> &type_id,

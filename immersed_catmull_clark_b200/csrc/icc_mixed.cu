@@ -34,11 +34,11 @@ namespace icc {
         if (_e != cudaSuccess) return ::icc::cuda_fail(_e, where); \
     } while (0)
 
-constexpr int kTcM = kEPB;        // 128 rows = the brick's elements
-constexpr int kTcN = 96;          // test DOFs 81 -> 96
-constexpr int kTcK = 88;          // trial DOFs 81 -> 88 = 11 MMAs of K = 8
-constexpr int kTcKSteps = kTcK / 8;
-constexpr int kBFl = kTcN * kTcK;  // floats per B term
+constexpr int kTcM = kEPB;             // 128 rows = the brick's elements
+constexpr int kTcN = 96;               // test DOFs: component c at rows c*32 + [0, 27)
+constexpr int kTcK = 96;               // trial DOFs: component c at columns c*32 + [0, 27)
+constexpr int kTcKSteps = kTcK / 8;    // 12 MMAs of K = 8 per term
+constexpr int kBFl = kTcN * kTcK;      // floats per B term
 constexpr uint32_t kBLbo = (kTcN / 8) * 128;  // bytes between K-adjacent core matrices of B
 constexpr uint32_t kSbo = 128;                // bytes between 8-row groups
 constexpr long long kWaitLimit = 1LL << 22;
@@ -48,17 +48,32 @@ __host__ __device__ __forceinline__ int canon(int row, int k, int rows) {
     return (k >> 2) * (rows / 8) * 32 + (row >> 3) * 32 + (row & 7) * 4 + (k & 3);
 }
 
+// Class of an element position along one direction of n elements: on open uniform knots the two
+// first and the two last elements restrict the B-splines differently, all others alike.
+__host__ __device__ __forceinline__ int pos_class(int e, int n) {
+    const int r = n - 1 - e;
+    return r < 2 ? 4 - r : (e < 2 ? e : 2);
+}
+
+// Every element of a uniform grid spans the same quadratics, so its local basis is a fixed
+// 3x3 recombination of the most frequent element's along each direction: N_e = R_d N_main.
+// Then K_e = R K_main R^T with R = (R_z (x) R_y (x) R_x) per component, and one MMA pass with
+// K_main serves every element: the operand gets R^T u_e, the result R (K_main R^T u_e).
+struct Xform {
+    float r[3][5][9];    // R of each direction and position class, row-major
+    unsigned nonid[3];   // bit k: class k is not the identity
+};
+
 struct MixedState {
     bool ready = false;
-    float4 *d_bmat = nullptr;        // [ntypes][2 terms][kBFl] canonical layout, hi then lo
+    float4 *d_bmat = nullptr;        // K_main split [hi, lo][kBFl] in the canonical layout
+    Xform xf{};
     float *d_scale32 = nullptr;
-    int *d_pass_start = nullptr, *d_pass_type = nullptr;
     float *d_patch32 = nullptr;
     float *d_rhs32 = nullptr, *d_x32 = nullptr, *d_r32 = nullptr, *d_p32 = nullptr, *d_ap32 = nullptr,
           *d_inv32 = nullptr, *d_xm32 = nullptr;   // xm32: masked input of the brick apply
     double *d_x64 = nullptr, *d_r64 = nullptr, *d_y64 = nullptr, *d_scalars = nullptr;
     int *d_err = nullptr;
-    int main_type = 0;               // most frequent pass type: pinned in B buffer 0
     PcgState *d_state = nullptr, *h_state = nullptr;
     double *h_scalars = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -71,27 +86,27 @@ struct MixedState {
 
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
 // One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (13 warps):
-//   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; split the current
-//     brick's gathered element vectors into TF32 hi/lo and store them as the A operand straight
-//     into TMEM (row m = element m = lane m), double-buffered in two A slots;
-//   warp 12 (MMA): keeps B = K_type hi/lo in shared memory (buffer 0 pinned to the grid's main
-//     element type, buffer 1 for the others, fetched with cp.async.bulk and prefetched while a
-//     main-type pass runs), issues the 33 tcgen05.mma (A from TMEM, B from shared memory) per
-//     type pass into one TMEM accumulator;
+//   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; per component,
+//     gather each element's 27 values, shift them by the element's centre value, apply R^T along
+//     the directions where the brick touches a boundary class, split into TF32 hi/lo and store
+//     them as the A operand straight into TMEM (row m = element m = lane m), in two A slots;
+//   warp 12 (MMA): holds B = K_main hi/lo in shared memory and issues the 36 tcgen05.mma (A from
+//     TMEM, B from shared memory) of a brick into the TMEM accumulator;
 //   warps 4-11 (epilogue, two groups of 4 taking alternate bricks): read the accumulator with
-//     tcgen05.ld, keep each row's own type pass, scale by s_e and sum the element results per
-//     patch node with warp shuffles (x, y) and a small shared buffer (z), then write the brick
-//     partials.
-// mbarriers: a_full/a_empty (A slots), d_full/d_empty (accumulator), b_full/b1_free (B buffers).
+//     tcgen05.ld and release it, apply R, scale by s_e and sum the element results per patch node
+//     with warp shuffles (x, y) and a small shared buffer (z), then write the brick partials.
+// mbarriers: a_full/a_empty (A slots), d_full (per epilogue group)/d_empty (accumulator), b_full.
 // Every wait is bounded; on time-out the CTA raises a shared abort flag, so all roles finish
 // promptly and the host reports ICC_TIMEOUT.
-constexpr int kPtThreads = 13 * 32;
-constexpr int kColSlot = 176;    // A slot s: hi at s*176 + [0,88), lo at s*176 + 88 + [0,88)
-constexpr int kColD = 352;       // accumulator: 96 columns
+constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24
+constexpr int kRoleThreads = kRoleWarps * 32;
+constexpr int kPtThreads = (2 * kRoleWarps + 1) * 32;
+constexpr int kColSlot = 2 * kTcK;     // A slot s: hi at s*192 + [0,96), lo at s*192 + 96 + [0,96)
+constexpr int kColD = 2 * kColSlot;    // accumulator: 96 columns at 384
 constexpr uint32_t kPtTmemCols = 512;
 constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
-constexpr int kPtSmem = (4 * kBFl + 2 * 3 * kPVol + 2 * kZFl) * 4;  // 161,280 B
-constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // one type, hi + lo
+constexpr int kPtSmem = (2 * kBFl + 2 * 3 * kPVol + 2 * kZFl) * 4;  // 99,648 B
+constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
     for (long long i = 0; i < kWaitLimit; ++i) {
@@ -119,64 +134,73 @@ __device__ __forceinline__ BrickBox brick_box(const Geom &g, int b) {
     return r;
 }
 
-// per-row data of one brick, loaded a brick ahead by the drain warps
-struct RowMeta {
-    int type, p0, p1, t0;
-    float scale;
-};
+// does any element of the brick along one direction (positions e0 .. e0 + cnt - 1) need R?
+__device__ __forceinline__ bool brick_needs(unsigned nonid, int e0, int cnt, int n) {
+    bool f = ((nonid >> 2) & 1u) != 0u;   // interior class: positions 2 .. n - 3
+    if (e0 < 2 || e0 + cnt > n - 2)
+        for (int i = 0; i < cnt; ++i) f |= ((nonid >> pos_class(e0 + i, n)) & 1u) != 0u;
+    return f;
+}
 
-__device__ __forceinline__ RowMeta row_meta(const Geom &g, int b, int r, const int *__restrict__ type_id,
-                                            const float *__restrict__ scale, const int *__restrict__ pass_start,
-                                            const int *__restrict__ pass_type) {
-    RowMeta m;
+// v <- M v along direction D of a 27-vector v[az*9 + ay*3 + ax], M = R (TR false) or R^T (TR true)
+template <int D, bool TR>
+__device__ __forceinline__ void xform_dir(float (&v)[27], const float *R) {
+    float m[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) m[3 * i + j] = TR ? R[3 * j + i] : R[3 * i + j];
+    constexpr int st = D == 0 ? 1 : (D == 1 ? 3 : 9);
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int i0 = D == 0 ? p * 9 + q * 3 : (D == 1 ? p * 9 + q : p * 3 + q);
+            const float a = v[i0], b = v[i0 + st], c = v[i0 + 2 * st];
+            v[i0] = fmaf(m[2], c, fmaf(m[1], b, m[0] * a));
+            v[i0 + st] = fmaf(m[5], c, fmaf(m[4], b, m[3] * a));
+            v[i0 + 2 * st] = fmaf(m[8], c, fmaf(m[7], b, m[6] * a));
+        }
+}
+
+__device__ __forceinline__ float row_scale(const Geom &g, int b, int r, const float *__restrict__ scale) {
     const BrickBox bb = brick_box(g, b);
     const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
-    m.type = -1;
-    m.scale = 0.f;
-    if (lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n) {
-        long long eg = (long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz));
-        m.type = type_id[eg];
-        m.scale = scale[eg];
-    }
-    m.p0 = pass_start[b];
-    m.p1 = pass_start[b + 1];
-    m.t0 = pass_type[m.p0];
-    return m;
+    if (lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n)
+        return scale[(long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz))];
+    return 0.f;
 }
 
 __global__ void __launch_bounds__(kPtThreads, 1)
-apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ scale, const int *__restrict__ type_id, const float4 *__restrict__ bmat,
-                int main_type, const int *__restrict__ pass_start, const int *__restrict__ pass_type,
-                float *__restrict__ patch_out, int *__restrict__ err, const PcgState *__restrict__ st) {
+apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ scale, const float4 *__restrict__ bmat,
+                const Xform xf, float *__restrict__ patch_out, int *__restrict__ err, const PcgState *__restrict__ st) {
     if (st && st->status != 0) return;
     extern __shared__ __align__(1024) float psm[];
-    float *sB = psm;                      // [2 buffers][hi, lo][kBFl]
-    float *sP = psm + 4 * kBFl;           // [2][3 * kPVol]
-    float *sZb = sP + 2 * 3 * kPVol;      // [2][kZFl] per-layer node partials
-    __shared__ __align__(8) uint64_t bars[10];
+    float *sB = psm;                      // [hi, lo][kBFl]
+    float *sP = psm + 2 * kBFl;           // [2][3 * kPVol]
+    float *sZb = sP + 2 * 3 * kPVol;      // [2][kZFl] per-layer node partials, by brick parity
+    __shared__ __align__(8) uint64_t bars[7];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
-    // d_full has one barrier per epilogue group: a group waits only for its own bricks' passes, so
-    // its parity waits never run two phases ahead of the barrier
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 7,
-             *b1_free = bars + 9;
+    __shared__ float s_r[3][5][9];
+    __shared__ unsigned s_nonid[3];
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *b_full = bars + 6;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
         tc::tmem_alloc(&tmem_base, kPtTmemCols);
         tc::tmem_relinquish();
     }
+    for (int i = tid; i < 3 * 5 * 9; i += kPtThreads) (&s_r[0][0][0])[i] = (&xf.r[0][0][0])[i];
+    if (tid < 3) s_nonid[tid] = xf.nonid[tid];
     if (tid == 0) {
-        tc::mbar_init(&a_full[0], 128);
-        tc::mbar_init(&a_full[1], 128);
+        tc::mbar_init(&a_full[0], kRoleThreads);
+        tc::mbar_init(&a_full[1], kRoleThreads);
         tc::mbar_init(&a_empty[0], 1);
         tc::mbar_init(&a_empty[1], 1);
-        tc::mbar_init(&d_full[0], 1);
-        tc::mbar_init(&d_full[1], 1);
-        tc::mbar_init(d_empty, 128);
-        tc::mbar_init(&b_full[0], 1);
-        tc::mbar_init(&b_full[1], 1);
-        tc::mbar_init(b1_free, 1);
+        tc::mbar_init(d_full, 1);
+        tc::mbar_init(d_empty, kRoleThreads);
+        tc::mbar_init(b_full, 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
@@ -186,22 +210,23 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     const uint32_t tmem = tmem_base;
     const int nmine = blockIdx.x < g.nbricks ? (g.nbricks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
-    if (warp < 4) {
+    if (warp < kRoleWarps) {
         // ------------------------------ builders ------------------------------
-        const int m = tid;
-        const int lx = m % kBX, ly = (m / kBX) % kBY, lz = m / (kBX * kBY);
-        const int base = (lz * kPY + ly) * kPX + lx;
-        // patch rows (c, pz, py) of kPX floats; thread m < 108 copies row m, in 8-byte pieces
+        // warp = 4 c + q: component c of the 32 elements of z-layer q (TMEM lanes 32 q ..)
+        const int c = warp >> 2, q = warp & 3;
+        const int lx = lane & 7, ly = lane >> 3;
+        const int base = c * kPVol + (q * kPY + ly) * kPX + lx;
+        // patch rows (c, pz, py) of kPX floats; thread tid < 108 copies row tid, in 8-byte pieces
         // when the row is whole and starts on an even float (always when the x control-point
         // count is even), else float by float
         auto load_patch = [&](int b, float *dst) {
-            if (m < 3 * kPZ * kPY) {
+            if (tid < 3 * kPZ * kPY) {
                 const BrickBox bb = brick_box(g, b);
-                const int c = m / (kPZ * kPY), py = m % kPY, pz = (m / kPY) % kPZ;
+                const int rc = tid / (kPZ * kPY), py = tid % kPY, pz = (tid / kPY) % kPZ;
                 const int gy = bb.y0 + py, gz = bb.z0 + pz;
-                float *drow = dst + m * kPX;
+                float *drow = dst + tid * kPX;
                 if (gy < g.cy && gz < g.cz) {
-                    const long long off = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
+                    const long long off = (long long)rc * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
                     const float *srow = x + off;
                     if (bb.x0 + kPX <= g.cx && !(off & 1)) {
 #pragma unroll
@@ -224,143 +249,131 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
             const int s = it & 1;
-            float *P = sP + s * 3 * kPVol;
             if (it + 1 < nmine) load_patch(b + gridDim.x, sP + ((it + 1) & 1) * 3 * kPVol);
             else tc::cp_async_commit();
-            tc::cp_async_wait<1>();
             const BrickBox bb = brick_box(g, b);
-            tc::named_sync(1, 128);
+            const bool fx = brick_needs(s_nonid[0], bb.x0, bb.ex_n, g.nx);
+            const bool fy = brick_needs(s_nonid[1], bb.y0, bb.ey_n, g.ny);
+            const bool fz = brick_needs(s_nonid[2], bb.z0, bb.ez_n, g.nz);
+            const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
+            tc::cp_async_wait<1>();
+            tc::named_sync(1, kRoleThreads);   // brick it's patch has landed for every builder
             if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
-            const bool valid = lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n;
-            const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kColSlot);
-            const float *Pm = P + base;
-            // Element-local shift: every K_e maps a constant per-component field to zero, so
-            // K_e (u_e - u_c 1_c) = K_e u_e with u_c the element's centre control value of
-            // component c.  The split operands then carry only the variation across the element,
-            // so the TF32 splitting error scales with that variation instead of with |u|, which
-            // matters for the smooth, low-energy vectors of a converging PCG.
-            float ctr[3];
+            const float *Pc = sP + s * 3 * kPVol + base;
+            float v[27];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) ctr[c] = valid ? Pm[c * kPVol + kPY * kPX + kPX + 1] : 0.f;
+            for (int a = 0; a < 27; ++a) v[a] = Pc[(a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
+            // Element-local shift: K_e maps a constant per-component field to zero, so subtracting
+            // the element's centre control value changes nothing in exact arithmetic while the
+            // split operands carry only the variation across the element; the TF32 splitting
+            // error then scales with that variation instead of with |u| (smooth, low-energy
+            // vectors of a converging PCG).  R^T maps constants to themselves.
+            const float ctr = v[13];
 #pragma unroll
-            for (int c8 = 0; c8 < kTcK / 8; ++c8) {
+            for (int a = 0; a < 27; ++a) v[a] = valid ? v[a] - ctr : 0.f;
+            if (fx) xform_dir<0, true>(v, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
+            if (fy) xform_dir<1, true>(v, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
+            if (fz) xform_dir<2, true>(v, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
+            const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(s * kColSlot + c * 32);
+#pragma unroll
+            for (int q8 = 0; q8 < 4; ++q8) {
                 float hi[8], lo[8];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int k = c8 * 8 + q;  // compile-time: the patch offset folds to an immediate
-                    float v = 0.f;
-                    if (k < 81) {
-                        const int c = k / 27, a = k % 27;
-                        if (valid) v = Pm[c * kPVol + (a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3] - ctr[c];
-                    }
-                    tc::split_tf32(v, hi[q], lo[q]);
-                }
-                tc::tmem_st8(trow + c8 * 8, hi);
-                tc::tmem_st8(trow + kTcK + c8 * 8, lo);
+                for (int j = 0; j < 8; ++j) tc::split_tf32(q8 * 8 + j < 27 ? v[q8 * 8 + j] : 0.f, hi[j], lo[j]);
+                tc::tmem_st8(col + q8 * 8, hi);
+                tc::tmem_st8(col + kTcK + q8 * 8, lo);
             }
             tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(&a_full[s]);
-            tc::named_sync(1, 128);   // everyone is done with P before the next prefetch reuses it
+            tc::named_sync(1, kRoleThreads);   // everyone is done with this patch before it is refilled
         }
         tc::cp_async_wait<0>();
-    } else if (warp < 12) {
+    } else if (warp < 2 * kRoleWarps) {
         // ------------------------------ epilogue ------------------------------
-        // Two groups of 4 warps take alternate bricks (group eg = brick parity), so one group can
-        // drain the accumulator for the next brick while the other still sums nodes.  Warp q4 of
-        // a group holds z-layer lz = q4 of its brick: lane = lx + 8 ly = element (lx, ly, q4) and
-        // TMEM lane 32 q4 + lane.  Node sums run in registers: along x with shuffles by 1 and 2
+        // warp = 12 + 4 c + q: component c of z-layer q; lane = lx + 8 ly = element (lx, ly, q)
+        // = TMEM lane 32 q + lane.  Node sums run in registers: along x with shuffles by 1 and 2
         // lanes, along y by 8 and 16 lanes; the 4 layers are combined through shared memory.
-        const int eg = (warp - 4) >> 2;
-        const int q4 = warp & 3;
-        const int r = q4 * 32 + lane;
+        const int et = tid - kRoleThreads;
+        const int c = (warp - kRoleWarps) >> 2, q = warp & 3;
+        const int r = q * 32 + lane;
         const int lx = lane & 7, ly = lane >> 3;
-        const uint32_t dcol = tmem + ((uint32_t)(q4 * 32) << 16) + kColD;
+        const uint32_t dcol = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kColD + c * 32);
         const unsigned FULL = 0xffffffffu;
-        float *sZ = sZb + eg * kZFl;
-        int j = 0;   // passes of this group's bricks so far (phases of d_full[eg])
+        float se_next = nmine > 0 ? row_scale(g, blockIdx.x, r, scale) : 0.f;
         for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
-            const int p0 = pass_start[b], p1 = pass_start[b + 1];
-            if ((it & 1) != eg) continue;
-            const RowMeta cur = row_meta(g, b, r, type_id, scale, pass_start, pass_type);
-            float res[81];
+            const float se = se_next;
+            float *sZ = sZb + (it & 1) * kZFl;
+            const BrickBox bb = brick_box(g, b);
+            const bool fx = brick_needs(s_nonid[0], bb.x0, bb.ex_n, g.nx);
+            const bool fy = brick_needs(s_nonid[1], bb.y0, bb.ey_n, g.ny);
+            const bool fz = brick_needs(s_nonid[2], bb.z0, bb.ez_n, g.nz);
+            const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
+            pt_wait(d_full, uint32_t(it) & 1u, &s_abort, err);
+            tc::fence_after_sync();
+            uint32_t dv[32];
+            tc::tmem_ld32(dcol, dv);
+            tc::tmem_wait_ld();
+            tc::fence_before_sync();
+            tc::mbar_arrive(d_empty);   // the accumulator is free for the next brick
+            if (it + 1 < nmine) se_next = row_scale(g, b + gridDim.x, r, scale);
+            float res[27];
 #pragma unroll
-            for (int n = 0; n < 81; ++n) res[n] = 0.f;
-            int t = cur.t0;
-            for (int pi = p0; pi < p1; ++pi, ++j) {
-                const int t_next = pi + 1 < p1 ? pass_type[pi + 1] : -1;
-                pt_wait(&d_full[eg], uint32_t(j) & 1u, &s_abort, err);
-                tc::fence_after_sync();
-                const bool take = cur.type == t;
-                const float se = cur.scale;
+            for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
+            if (fx) xform_dir<0, false>(res, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
+            if (fy) xform_dir<1, false>(res, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
+            if (fz) xform_dir<2, false>(res, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    uint32_t v[32];
-                    tc::tmem_ld32(dcol + ch * 32, v);
-                    tc::tmem_wait_ld();
+            for (int a = 0; a < 27; ++a) res[a] *= se;
+            // x, in place: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2) in res[o]; lanes
+            // lx = 7 also carry px = 8 (v[1](7) + v[2](6)) in res[o+1] and px = 9 (v[2](7)) in res[o+2]
 #pragma unroll
-                    for (int n = 0; n < 32; ++n)
-                        if (ch * 32 + n < 81) res[ch * 32 + n] = take ? se * __uint_as_float(v[n]) : res[ch * 32 + n];
+            for (int az = 0; az < 3; ++az)
+#pragma unroll
+                for (int ay = 0; ay < 3; ++ay) {
+                    const int o = 3 * ay + 9 * az;
+                    const float a0 = res[o], a1 = res[o + 1], a2 = res[o + 2];
+                    const float u1 = __shfl_up_sync(FULL, a1, 1), u2 = __shfl_up_sync(FULL, a2, 2);
+                    const float w1 = __shfl_up_sync(FULL, a2, 1);
+                    res[o] = (a0 + (lx >= 1 ? u1 : 0.f)) + (lx >= 2 ? u2 : 0.f);
+                    res[o + 1] = a1 + (lx >= 1 ? w1 : 0.f);
                 }
-                tc::fence_before_sync();
-                tc::mbar_arrive(d_empty);   // the accumulator is free for the next pass
-                t = t_next;
-            }
-            tc::named_sync(2 + eg, 128);   // this group's previous z-sum is done with sZ
+            // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also carry
+            // py = 4 and py = 5.  Results are this layer's partials for z-offset az.
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                // x: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2); lanes lx = 7 also
-                // carry px = 8 (v[1](7) + v[2](6)) and px = 9 (v[2](7)).  q = az*3 + ay.
-                float X[9], X8[9], X9[9];
+            for (int az = 0; az < 3; ++az)
 #pragma unroll
-                for (int az = 0; az < 3; ++az)
-#pragma unroll
-                    for (int ay = 0; ay < 3; ++ay) {
-                        const int q = az * 3 + ay, o = c * 27 + 3 * ay + 9 * az;
-                        const float a0 = res[o], a1 = res[o + 1], a2 = res[o + 2];
-                        const float u1 = __shfl_up_sync(FULL, a1, 1), u2 = __shfl_up_sync(FULL, a2, 2);
-                        const float w1 = __shfl_up_sync(FULL, a2, 1);
-                        X[q] = (a0 + (lx >= 1 ? u1 : 0.f)) + (lx >= 2 ? u2 : 0.f);
-                        X8[q] = a1 + (lx >= 1 ? w1 : 0.f);
-                        X9[q] = a2;
-                    }
-                // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also
-                // carry py = 4 and py = 5.  Results are this layer's partials for z-offset az.
-#pragma unroll
-                for (int az = 0; az < 3; ++az)
-#pragma unroll
-                    for (int var = 0; var < 3; ++var) {
-                        const float *V = var == 0 ? X : (var == 1 ? X8 : X9);
-                        const int q = az * 3;
-                        const float a0 = V[q], a1 = V[q + 1], a2 = V[q + 2];
-                        const float s1 = __shfl_up_sync(FULL, a1, 8), s2 = __shfl_up_sync(FULL, a2, 16);
-                        const float t1 = __shfl_up_sync(FULL, a2, 8);
-                        const float yv = (a0 + (ly >= 1 ? s1 : 0.f)) + (ly >= 2 ? s2 : 0.f);
-                        const float y4 = a1 + (ly >= 1 ? t1 : 0.f);
-                        const int px = var == 0 ? lx : 7 + var;
-                        if (var == 0 || lx == 7) {
-                            float *zb = sZ + (((q4 * 3 + az) * 3 + c) * kPY) * kPX + px;
-                            zb[ly * kPX] = yv;
-                            if (ly == 3) {
-                                zb[4 * kPX] = y4;
-                                zb[5 * kPX] = a2;
-                            }
+                for (int var = 0; var < 3; ++var) {
+                    const float a0 = res[9 * az + var], a1 = res[9 * az + 3 + var], a2 = res[9 * az + 6 + var];
+                    const float s1 = __shfl_up_sync(FULL, a1, 8), s2 = __shfl_up_sync(FULL, a2, 16);
+                    const float t1 = __shfl_up_sync(FULL, a2, 8);
+                    const float yv = (a0 + (ly >= 1 ? s1 : 0.f)) + (ly >= 2 ? s2 : 0.f);
+                    const float y4 = a1 + (ly >= 1 ? t1 : 0.f);
+                    const int px = var == 0 ? lx : 7 + var;
+                    if (var == 0 || lx == 7) {
+                        float *zb = sZ + (((q * 3 + az) * 3 + c) * kPY) * kPX + px;
+                        zb[ly * kPX] = yv;
+                        if (ly == 3) {
+                            zb[4 * kPX] = y4;
+                            zb[5 * kPX] = a2;
                         }
                     }
-            }
-            tc::named_sync(2 + eg, 128);
+                }
+            // all layers of brick it are in sZ[it & 1]; every z-sum of brick it - 1 (which read
+            // the other buffer) finished before its thread reached this barrier
+            tc::named_sync(2, kRoleThreads);
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
             float *ob = patch_out + (size_t)b * 3 * kPVol;
-            for (int i = r; i < 3 * kPVol; i += 128) {
-                const int c = i / kPVol, rem = i - c * kPVol;
+            for (int i = et; i < 3 * kPVol; i += kRoleThreads) {
+                const int ci = i / kPVol, rem = i - ci * kPVol;
                 const int pz = rem / (kPX * kPY), pyx = rem - pz * (kPX * kPY);
                 float sum = 0.f;
 #pragma unroll
                 for (int az = 0; az < 3; ++az) {
                     const int lz = pz - az;
-                    if (lz >= 0 && lz < kBZ) sum += sZ[((lz * 3 + az) * 3 + c) * (kPY * kPX) + pyx];
+                    if (lz >= 0 && lz < kBZ) sum += sZ[((lz * 3 + az) * 3 + ci) * (kPY * kPX) + pyx];
                 }
                 ob[i] = sum;
             }
@@ -368,74 +381,33 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     } else if (lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
         constexpr uint32_t idesc = tc::idesc_tf32(kTcM, kTcN);
-        tc::mbar_arrive_expect_tx(&b_full[0], kBBytes);
-        tc::bulk_g2s(sB, bmat + (size_t)main_type * (2 * kBFl / 4), kBBytes, &b_full[0]);
-        pt_wait(&b_full[0], 0u, &s_abort, err);
-        // descriptors of K step 0 for both B buffers (hi and lo terms); the shared-memory window
-        // is below 256 KB, so adding a step's offset never carries out of the address field
-        const uint64_t dbh0_base = tc::make_desc(sB, kBLbo, kSbo), dbl0_base = tc::make_desc(sB + kBFl, kBLbo, kSbo);
-        const uint64_t dbh1_base = tc::make_desc(sB + 2 * kBFl, kBLbo, kSbo),
-                       dbl1_base = tc::make_desc(sB + 3 * kBFl, kBLbo, kSbo);
-        int tag1 = -1;             // type held (or being fetched) in B buffer 1
-        bool pending = false;      // a fetch into buffer 1 has not been waited for yet
-        uint32_t b1_loads = 0, b1_uses = 0;
-        auto fetch1 = [&](int t) {
-            if (b1_uses > 0) pt_wait(b1_free, (b1_uses - 1) & 1u, &s_abort, err);  // no MMA reads buffer 1
-            tc::mbar_arrive_expect_tx(&b_full[1], kBBytes);
-            tc::bulk_g2s(sB + 2 * kBFl, bmat + (size_t)t * (2 * kBFl / 4), kBBytes, &b_full[1]);
-            tag1 = t;
-            pending = true;
-            b1_loads++;
-        };
-        int j = 0;
+        tc::mbar_arrive_expect_tx(b_full, kBBytes);
+        tc::bulk_g2s(sB, bmat, kBBytes, b_full);
+        pt_wait(b_full, 0u, &s_abort, err);
+        // descriptors of K step 0 (hi and lo terms); the shared-memory window is below 256 KB,
+        // so adding a step's offset never carries out of the address field
+        const uint64_t dbh0 = tc::make_desc(sB, kBLbo, kSbo), dbl0 = tc::make_desc(sB + kBFl, kBLbo, kSbo);
         for (int it = 0; it < nmine; ++it) {
-            const int b = blockIdx.x + it * gridDim.x;
             const int s = it & 1;
-            const int p0 = pass_start[b], p1 = pass_start[b + 1];
-            const int bn = b + gridDim.x;
-            const int pn = it + 1 < nmine ? pass_start[bn] : -1;
-            int t = pass_type[p0];
             pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
-            for (int pi = p0; pi < p1; ++pi, ++j) {
-                const int t_next = pi + 1 < p1 ? pass_type[pi + 1] : (pn >= 0 ? pass_type[pn] : -1);
-                // the previous pass has been drained: no MMA still writes the accumulator
-                if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
-                int buf = 0;
-                if (t != main_type) {
-                    buf = 1;
-                    if (tag1 != t) fetch1(t);
-                    if (pending) {
-                        pt_wait(&b_full[1], (b1_loads - 1) & 1u, &s_abort, err);
-                        pending = false;
-                    }
-                }
-                tc::fence_after_sync();
-                const uint64_t dbh0 = buf ? dbh1_base : dbh0_base, dbl0 = buf ? dbl1_base : dbl0_base;
-                const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
+            // the previous brick has been drained: no MMA still writes the accumulator
+            if (it >= 1) pt_wait(d_empty, uint32_t(it - 1) & 1u, &s_abort, err);
+            tc::fence_after_sync();
+            const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
 #pragma unroll
-                for (int ks = 0; ks < kTcKSteps; ++ks) {
-                    // one K step of 8 = two core-matrix columns: advance the start address field
-                    const uint64_t dk = (uint64_t)(ks * 2 * kBLbo) >> 4;
-                    const uint64_t dbh = dbh0 + dk, dbl = dbl0 + dk;
-                    const uint32_t ah = acol + ks * 8, al = acol + kTcK + ks * 8;
-                    tc::mma_tf32_ts(tmem + kColD, al, dbh, idesc, ks > 0 ? 1u : 0u);
-                    tc::mma_tf32_ts(tmem + kColD, ah, dbl, idesc, 1u);
-                    tc::mma_tf32_ts(tmem + kColD, ah, dbh, idesc, 1u);
-                }
-                tc::mma_commit(&d_full[it & 1]);
-                if (buf == 1) {
-                    tc::mma_commit(b1_free);
-                    b1_uses++;
-                } else if (t_next >= 0 && t_next != main_type && t_next != tag1) {
-                    fetch1(t_next);  // overlaps this main-type pass
-                }
-                t = t_next;
+            for (int ks = 0; ks < kTcKSteps; ++ks) {
+                // one K step of 8 = two core-matrix columns: advance the start address field
+                const uint64_t dk = (uint64_t)(ks * 2 * kBLbo) >> 4;
+                const uint64_t dbh = dbh0 + dk, dbl = dbl0 + dk;
+                const uint32_t ah = acol + ks * 8, al = acol + kTcK + ks * 8;
+                tc::mma_tf32_ts(tmem + kColD, al, dbh, idesc, ks > 0 ? 1u : 0u);
+                tc::mma_tf32_ts(tmem + kColD, ah, dbl, idesc, 1u);
+                tc::mma_tf32_ts(tmem + kColD, ah, dbh, idesc, 1u);
             }
+            tc::mma_commit(d_full);
             tc::mma_commit(&a_empty[s]);
         }
-        if (j >= 1) pt_wait(d_empty, uint32_t(j - 1) & 1u, &s_abort, err);
-        if (b1_uses > 0) pt_wait(b1_free, (b1_uses - 1) & 1u, &s_abort, err);
-        if (pending) pt_wait(&b_full[1], (b1_loads - 1) & 1u, &s_abort, err);
+        if (nmine >= 1) pt_wait(d_empty, uint32_t(nmine - 1) & 1u, &s_abort, err);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -527,58 +499,150 @@ static int dalloc(T **p, size_t count, const char *what) {
     return ICC_OK;
 }
 
+static bool inv3(const double *a, double *o) {
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    if (!(std::fabs(det) > 1e-300)) return false;
+    o[0] = (a[4] * a[8] - a[5] * a[7]) / det;
+    o[1] = (a[2] * a[7] - a[1] * a[8]) / det;
+    o[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+    o[3] = (a[5] * a[6] - a[3] * a[8]) / det;
+    o[4] = (a[0] * a[8] - a[2] * a[6]) / det;
+    o[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+    o[6] = (a[3] * a[7] - a[4] * a[6]) / det;
+    o[7] = (a[1] * a[6] - a[0] * a[7]) / det;
+    o[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+    return true;
+}
+
+// out = (R_z (x) R_y (x) R_x) in per component, on 81-vectors with element strides sin / sout
+static void apply_r3(const double *Rx, const double *Ry, const double *Rz, const double *in, int sin, double *out,
+                     int sout) {
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 27; ++a) {
+            const int ax = a % 3, ay = (a / 3) % 3, az = a / 9;
+            double s = 0.0;
+            for (int b = 0; b < 27; ++b) {
+                const int bx = b % 3, by = (b / 3) % 3, bz = b / 9;
+                s += Rz[az * 3 + bz] * Ry[ay * 3 + by] * Rx[ax * 3 + bx] * in[(c * 27 + b) * sin];
+            }
+            out[(c * 27 + a) * sout] = s;
+        }
+}
+
+// Single-pass set-up: the main (most frequent) element type, the 1-D transforms R of every
+// direction and position class, and the check that each element type's matrix equals
+// R K_main R^T (to 1e-9 of max |K_main|); returns the main type or -1 with the error set.
+static int setup_xform(const Op &op, Xform &xf) {
+    const Geom &g = op.g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    std::vector<long long> count((size_t)op.ntypes, 0);
+    for (int32_t t : op.host_type_id) count[(size_t)t]++;
+    int mt = 0;
+    for (int t = 1; t < op.ntypes; ++t)
+        if (count[(size_t)t] > count[(size_t)mt]) mt = t;
+    long long e0 = 0;
+    while (op.host_type_id[(size_t)e0] != mt) ++e0;
+    const int pos0[3] = {int(e0 % g.nx), int((e0 / g.nx) % g.ny), int(e0 / ((long long)g.nx * g.ny))};
+    double R[3][5][9];
+    for (int d = 0; d < 3; ++d) {
+        const std::vector<int> &t1d = op.host_type1d[d];
+        if ((int)t1d.size() != n[d] || op.host_basis1d[d].empty()) {
+            set_error(ICC_BAD_ARG, "tensor-core path: space without 1-D basis data");
+            return -1;
+        }
+        const int main1d = t1d[(size_t)pos0[d]];
+        double vinv[9];
+        if (!inv3(op.host_basis1d[d][(size_t)main1d].data(), vinv)) {
+            set_error(ICC_BAD_ARG, "tensor-core path: singular 1-D basis");
+            return -1;
+        }
+        xf.nonid[d] = 0;
+        for (int k = 0; k < 5; ++k) {
+            int rep = -1;
+            for (int e = 0; e < n[d] && rep < 0; ++e)
+                if (pos_class(e, n[d]) == k) rep = e;
+            for (int i = 0; i < 9; ++i) R[d][k][i] = (i % 4 == 0) ? 1.0 : 0.0;
+            if (rep >= 0 && t1d[(size_t)rep] != main1d) {
+                const double *vt = op.host_basis1d[d][(size_t)t1d[(size_t)rep]].data();
+                for (int i = 0; i < 3; ++i)
+                    for (int b = 0; b < 3; ++b) {
+                        double s = 0.0;
+                        for (int q = 0; q < 3; ++q) s += vt[3 * i + q] * vinv[3 * q + b];
+                        R[d][k][3 * i + b] = s;
+                    }
+                // a split of numerically equal 1-D types is still the identity
+                double dev = 0.0;
+                for (int i = 0; i < 9; ++i) dev = std::fmax(dev, std::fabs(R[d][k][i] - ((i % 4 == 0) ? 1.0 : 0.0)));
+                if (dev > 1e-12) xf.nonid[d] |= 1u << k;
+                else
+                    for (int i = 0; i < 9; ++i) R[d][k][i] = (i % 4 == 0) ? 1.0 : 0.0;
+            }
+            for (int i = 0; i < 9; ++i) xf.r[d][k][i] = float(R[d][k][i]);
+        }
+    }
+    // every element's matrix must be the transformed main matrix of its class triple (the 1-D
+    // grouping rounds matrices to 1e-12, so a class may hold several numerically equal types)
+    std::vector<char> seen((size_t)125 * op.ntypes, 0);
+    for (int ez = 0; ez < g.nz; ++ez)
+        for (int ey = 0; ey < g.ny; ++ey)
+            for (int ex = 0; ex < g.nx; ++ex) {
+                const int key = pos_class(ex, g.nx) + 5 * (pos_class(ey, g.ny) + 5 * pos_class(ez, g.nz));
+                const int t = op.host_type_id[(size_t)ex + (size_t)g.nx * ((size_t)ey + (size_t)g.ny * ez)];
+                seen[(size_t)key * op.ntypes + t] = 1;
+            }
+    const double *K0 = op.host_ktypes.data() + (size_t)mt * 81 * 81;
+    double kmax = 0.0;
+    for (int i = 0; i < 81 * 81; ++i) kmax = std::fmax(kmax, std::fabs(K0[i]));
+    std::vector<double> t1(81 * 81), t2(81 * 81);
+    for (int key = 0; key < 125; ++key) {
+        bool any = false;
+        for (int t = 0; t < op.ntypes; ++t) any |= seen[(size_t)key * op.ntypes + t] != 0;
+        if (!any) continue;
+        const double *Rx = R[0][key % 5], *Ry = R[1][(key / 5) % 5], *Rz = R[2][key / 25];
+        for (int j = 0; j < 81; ++j) apply_r3(Rx, Ry, Rz, K0 + j, 81, t1.data() + j, 81);        // R K0
+        for (int i = 0; i < 81; ++i) apply_r3(Rx, Ry, Rz, t1.data() + i * 81, 1, t2.data() + i * 81, 1);  // (R K0) R^T
+        for (int t = 0; t < op.ntypes; ++t) {
+            if (!seen[(size_t)key * op.ntypes + t]) continue;
+            const double *Kt = op.host_ktypes.data() + (size_t)t * 81 * 81;
+            double dmax = 0.0;
+            for (int i = 0; i < 81 * 81; ++i) dmax = std::fmax(dmax, std::fabs(t2[(size_t)i] - Kt[i]));
+            if (!(dmax <= 1e-9 * kmax)) {
+                set_error(ICC_BAD_ARG, "tensor-core path: an element matrix is not the transformed main element "
+                                       "matrix (element matrices must come from the space's own bases)");
+                return -1;
+            }
+        }
+    }
+    return mt;
+}
+
 static int mixed_init(Op &op) {
     if (op.mixed && op.mixed->ready) return ICC_OK;
     if (!op.mixed) op.mixed = new MixedState();
     MixedState &ms = *op.mixed;
-    const int nt = op.ntypes;
-    // element matrices split into TF32 hi/lo in the canonical layout
-    std::vector<float> bm((size_t)nt * 2 * kBFl, 0.f);
-    for (int t = 0; t < nt; ++t) {
-        const double *K = op.host_ktypes.data() + (size_t)t * 81 * 81;
-        float *hi = bm.data() + (size_t)t * 2 * kBFl, *lo = hi + kBFl;
+    const int mt = setup_xform(op, ms.xf);
+    if (mt < 0) return ICC_BAD_ARG;
+    // the main element matrix split into TF32 hi/lo in the canonical layout, component c of the
+    // test (row) and trial (column) DOFs at c*32 + [0, 27)
+    std::vector<float> bm((size_t)2 * kBFl, 0.f);
+    {
+        const double *K = op.host_ktypes.data() + (size_t)mt * 81 * 81;
+        float *hi = bm.data(), *lo = hi + kBFl;
         for (int n = 0; n < 81; ++n)
             for (int k = 0; k < 81; ++k) {
-                double v = K[n * 81 + k];
-                float h = host_tf32(float(v));
-                float l = host_tf32(float(v - double(h)));
-                hi[canon(n, k, kTcN)] = h;
-                lo[canon(n, k, kTcN)] = l;
+                const double v = K[n * 81 + k];
+                const float h = host_tf32(float(v));
+                const float l = host_tf32(float(v - double(h)));
+                const int nr = (n / 27) * 32 + n % 27, kc = (k / 27) * 32 + k % 27;
+                hi[canon(nr, kc, kTcN)] = h;
+                lo[canon(nr, kc, kTcN)] = l;
             }
     }
     int rc;
     if ((rc = dalloc(&ms.d_bmat, bm.size() / 4, "alloc tc matrices"))) return rc;
     ICC_CUDA(cudaMemcpy(ms.d_bmat, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice), "copy tc matrices");
-    // per brick: distinct element types in first-appearance order (one MMA pass each)
-    std::vector<int> pstart(1, 0), ptype;
     const Geom &g = op.g;
-    for (int b = 0; b < g.nbricks; ++b) {
-        int bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / (g.nbx * g.nby);
-        std::vector<int> seen;
-        for (int lz = 0; lz < kBZ && bzi * kBZ + lz < g.nz; ++lz)
-            for (int ly = 0; ly < kBY && byi * kBY + ly < g.ny; ++ly)
-                for (int lx = 0; lx < kBX && bxi * kBX + lx < g.nx; ++lx) {
-                    int64_t e = (bxi * kBX + lx) + (int64_t)g.nx * ((byi * kBY + ly) + (int64_t)g.ny * (bzi * kBZ + lz));
-                    int t = op.host_type_id[(size_t)e];
-                    bool found = false;
-                    for (int v : seen) found |= v == t;
-                    if (!found) seen.push_back(t);
-                }
-        for (int t : seen) ptype.push_back(t);
-        pstart.push_back(int(ptype.size()));
-    }
-    {
-        std::vector<int> count((size_t)op.ntypes, 0);
-        for (int t : ptype) count[(size_t)t]++;
-        int best = 0;
-        for (int t = 1; t < op.ntypes; ++t)
-            if (count[(size_t)t] > count[(size_t)best]) best = t;
-        ms.main_type = best;
-    }
-    if ((rc = dalloc(&ms.d_pass_start, pstart.size(), "alloc passes"))) return rc;
-    if ((rc = dalloc(&ms.d_pass_type, ptype.size(), "alloc passes"))) return rc;
-    ICC_CUDA(cudaMemcpy(ms.d_pass_start, pstart.data(), pstart.size() * 4, cudaMemcpyHostToDevice), "copy passes");
-    ICC_CUDA(cudaMemcpy(ms.d_pass_type, ptype.data(), ptype.size() * 4, cudaMemcpyHostToDevice), "copy passes");
     const size_t n = (size_t)op.ndof;
     if ((rc = dalloc(&ms.d_scale32, (size_t)op.nel, "alloc mixed"))) return rc;
     if ((rc = dalloc(&ms.d_patch32, (size_t)g.nbricks * 3 * kPVol, "alloc mixed"))) return rc;
@@ -604,8 +668,8 @@ void mixed_release(Op &op) {
     if (!op.mixed) return;
     MixedState &ms = *op.mixed;
     if (ms.graph) cudaGraphExecDestroy(ms.graph);
-    void *bufs[] = {ms.d_bmat, ms.d_scale32, ms.d_pass_start, ms.d_pass_type, ms.d_patch32, ms.d_rhs32, ms.d_x32,
-                    ms.d_r32, ms.d_p32, ms.d_ap32, ms.d_inv32, ms.d_x64, ms.d_r64, ms.d_y64, ms.d_scalars,
+    void *bufs[] = {ms.d_bmat, ms.d_scale32, ms.d_patch32, ms.d_rhs32, ms.d_x32, ms.d_r32, ms.d_p32,
+                    ms.d_ap32, ms.d_inv32, ms.d_xm32, ms.d_x64, ms.d_r64, ms.d_y64, ms.d_scalars,
                     ms.d_err, ms.d_state};
     for (void *p : bufs)
         if (p) cudaFree(p);
@@ -633,8 +697,7 @@ __global__ void mask_copy_kernel(long long n, const float *__restrict__ x, const
 static void launch_apply_tc(Op &op, const float *xin, const PcgState *st) {
     MixedState &ms = *op.mixed;
     const int grid = std::min(op.num_sms, op.g.nbricks);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, op.d_type_id, ms.d_bmat,
-                                                              ms.main_type, ms.d_pass_start, ms.d_pass_type,
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, ms.d_bmat, ms.xf,
                                                               ms.d_patch32, ms.d_err, st);
 }
 

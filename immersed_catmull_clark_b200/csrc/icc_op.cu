@@ -303,6 +303,10 @@ int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type
     if ((rc = dev_alloc(&d_type_id, (size_t)nel, "alloc type_id"))) return rc;
     ICC_CUDA(cudaMemcpy(d_type_id, type_id, (size_t)nel * 4, cudaMemcpyHostToDevice), "copy type_id");
     host_type_id.assign(type_id, type_id + nel);
+    for (int d = 0; d < 3; ++d) {
+        host_type1d[d] = s.type1d[d];
+        host_basis1d[d] = s.basis1d[d];
+    }
 
     // brick tile plan: per brick, its elements grouped by type (first-appearance order) and cut
     // into warp tiles of 16 (255 marks an empty row)

@@ -97,6 +97,7 @@ struct Dir1d {
     std::vector<Mat1d> distinct;   // distinct 1-D matrix quadruples, first-appearance order
     std::vector<int> type_of;      // 1-D type of every element
     std::vector<int> first_cp;     // first control point of every element
+    std::vector<std::array<double, 9>> basis;  // basis values of each distinct type (Space::basis1d)
 };
 
 Dir1d build_direction(int nel, double length) {
@@ -154,6 +155,14 @@ Dir1d build_direction(int nel, double length) {
             t = int(out.distinct.size());
             seen.emplace(key, t);
             out.distinct.push_back(per[e]);
+            std::array<double, 9> bv;
+            const double a = br[e], h = br[e + 1] - br[e];
+            for (int q = 0; q < 3; ++q) {
+                double v[3], dv[3];
+                quadratic_basis(kn, a + 0.5 * (xg[q] + 1.0) * h, v, dv);
+                for (int i = 0; i < 3; ++i) bv[3 * i + q] = v[i];
+            }
+            out.basis.push_back(bv);
         } else {
             t = it->second;
         }
@@ -179,6 +188,7 @@ bool Space::init(const double bounds[6], const int64_t nsub[3]) {
         Dir1d dd = build_direction(int(nel_dir[d]), len[d]);
         mats1d[d] = dd.distinct;
         type1d[d] = dd.type_of;
+        basis1d[d] = dd.basis;
         for (int e = 0; e < int(nel_dir[d]); ++e)
             if (dd.first_cp[size_t(e)] != e) return false;  // uniform grid: element e starts at cp e
     }
