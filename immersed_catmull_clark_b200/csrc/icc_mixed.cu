@@ -95,17 +95,19 @@ struct MixedState {
 //   warps 4-11 (epilogue, two groups of 4 taking alternate bricks): read the accumulator with
 //     tcgen05.ld and release it, apply R, scale by s_e and sum the element results per patch node
 //     with warp shuffles (x, y) and a small shared buffer (z), then write the brick partials.
-// mbarriers: a_full/a_empty (A slots), d_full (per epilogue group)/d_empty (accumulator), b_full.
+// mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full.
 // Every wait is bounded; on time-out the CTA raises a shared abort flag, so all roles finish
 // promptly and the host reports ICC_TIMEOUT.
 constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24
 constexpr int kRoleThreads = kRoleWarps * 32;
 constexpr int kPtThreads = (2 * kRoleWarps + 1) * 32;
-constexpr int kColSlot = 2 * kTcK;     // A slot s: hi at s*192 + [0,96), lo at s*192 + 96 + [0,96)
-constexpr int kColD = 2 * kColSlot;    // accumulator: 96 columns at 384
+constexpr int kColSlot = kTcK;         // A_hi slot s: TMEM columns s*96 + [0,96)
+constexpr int kColD = 2 * kColSlot;    // accumulator buffer d: TMEM columns 192 + d*96 + [0,96)
+constexpr int kAloFl = kTcM * kTcK;    // A_lo slot (shared memory, canonical K-major): floats
+constexpr uint32_t kALbo = (kTcM / 8) * 128;  // bytes between K-adjacent core matrices of A_lo
 constexpr uint32_t kPtTmemCols = 512;
 constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
-constexpr int kPtSmem = (2 * kBFl + 2 * 3 * kPVol + 2 * kZFl) * 4;  // 99,648 B
+constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * 3 * kPVol + 2 * kZFl) * 4;  // 202,272 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
@@ -134,11 +136,49 @@ __device__ __forceinline__ BrickBox brick_box(const Geom &g, int b) {
     return r;
 }
 
+// Walks the bricks b, b + step, b + 2 step, ... of a persistent CTA without integer divisions in
+// the loop (the step is split into per-direction increments once).
+struct BrickWalk {
+    int bx, by, bz, sx, sy, sz;
+    __device__ __forceinline__ void init(const Geom &g, int b, int step) {
+        bx = b % g.nbx;
+        by = (b / g.nbx) % g.nby;
+        bz = b / (g.nbx * g.nby);
+        sx = step % g.nbx;
+        sy = (step / g.nbx) % g.nby;
+        sz = step / (g.nbx * g.nby);
+    }
+    __device__ __forceinline__ void next(const Geom &g) {
+        bx += sx;
+        const int cy = bx >= g.nbx ? 1 : 0;
+        bx -= cy * g.nbx;
+        by += sy + cy;
+        const int cz = by >= g.nby ? 1 : 0;
+        by -= cz * g.nby;
+        bz += sz + cz;
+    }
+    __device__ __forceinline__ BrickBox box(const Geom &g) const {
+        BrickBox r;
+        r.x0 = bx * kBX;
+        r.y0 = by * kBY;
+        r.z0 = bz * kBZ;
+        r.ex_n = min(kBX, g.nx - r.x0);
+        r.ey_n = min(kBY, g.ny - r.y0);
+        r.ez_n = min(kBZ, g.nz - r.z0);
+        return r;
+    }
+};
+
 // does any element of the brick along one direction (positions e0 .. e0 + cnt - 1) need R?
+// Only the interior class (positions 2 .. n-3) and the positions 0, 1, n-2, n-1 can differ.
 __device__ __forceinline__ bool brick_needs(unsigned nonid, int e0, int cnt, int n) {
-    bool f = ((nonid >> 2) & 1u) != 0u;   // interior class: positions 2 .. n - 3
-    if (e0 < 2 || e0 + cnt > n - 2)
-        for (int i = 0; i < cnt; ++i) f |= ((nonid >> pos_class(e0 + i, n)) & 1u) != 0u;
+    const int e1 = e0 + cnt - 1;
+    bool f = ((nonid >> 2) & 1u) != 0u && e1 >= 2 && e0 <= n - 3;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int p = k < 2 ? k : n - 4 + k;
+        if (p >= e0 && p <= e1 && p >= 0) f |= ((nonid >> pos_class(p, n)) & 1u) != 0u;
+    }
     return f;
 }
 
@@ -163,8 +203,7 @@ __device__ __forceinline__ void xform_dir(float (&v)[27], const float *R) {
         }
 }
 
-__device__ __forceinline__ float row_scale(const Geom &g, int b, int r, const float *__restrict__ scale) {
-    const BrickBox bb = brick_box(g, b);
+__device__ __forceinline__ float row_scale(const Geom &g, const BrickBox &bb, int r, const float *__restrict__ scale) {
     const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
     if (lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n)
         return scale[(long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz))];
@@ -177,14 +216,15 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     if (st && st->status != 0) return;
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
-    float *sP = psm + 2 * kBFl;           // [2][3 * kPVol]
-    float *sZb = sP + 2 * 3 * kPVol;      // [2][kZFl] per-layer node partials, by brick parity
-    __shared__ __align__(8) uint64_t bars[7];
+    float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
+    float *sP = sAlo + 2 * kAloFl;        // [3][3 * kPVol] input patches
+    float *sZb = sP + 3 * 3 * kPVol;      // [2][kZFl] per-layer node partials, by brick parity
+    __shared__ __align__(8) uint64_t bars[9];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
     __shared__ float s_r[3][5][9];
     __shared__ unsigned s_nonid[3];
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 5, *b_full = bars + 6;
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
@@ -198,8 +238,10 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         tc::mbar_init(&a_full[1], kRoleThreads);
         tc::mbar_init(&a_empty[0], 1);
         tc::mbar_init(&a_empty[1], 1);
-        tc::mbar_init(d_full, 1);
-        tc::mbar_init(d_empty, kRoleThreads);
+        tc::mbar_init(&d_full[0], 1);
+        tc::mbar_init(&d_full[1], 1);
+        tc::mbar_init(&d_empty[0], kRoleThreads);
+        tc::mbar_init(&d_empty[1], kRoleThreads);
         tc::mbar_init(b_full, 1);
         tc::fence_mbar_init();
         s_abort = 0;
@@ -219,9 +261,8 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         // patch rows (c, pz, py) of kPX floats; thread tid < 108 copies row tid, in 8-byte pieces
         // when the row is whole and starts on an even float (always when the x control-point
         // count is even), else float by float
-        auto load_patch = [&](int b, float *dst) {
+        auto load_patch = [&](const BrickBox &bb, float *dst) {
             if (tid < 3 * kPZ * kPY) {
-                const BrickBox bb = brick_box(g, b);
                 const int rc = tid / (kPZ * kPY), py = tid % kPY, pz = (tid / kPY) % kPZ;
                 const int gy = bb.y0 + py, gz = bb.z0 + pz;
                 float *drow = dst + tid * kPX;
@@ -245,22 +286,30 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             }
             tc::cp_async_commit();
         };
-        if (nmine > 0) load_patch(blockIdx.x, sP);
-        for (int it = 0; it < nmine; ++it) {
-            const int b = blockIdx.x + it * gridDim.x;
-            const int s = it & 1;
-            if (it + 1 < nmine) load_patch(b + gridDim.x, sP + ((it + 1) & 1) * 3 * kPVol);
+        // three patch buffers: brick it + 2 is fetched while brick it is built
+        BrickWalk wc, wl;
+        wc.init(g, blockIdx.x, gridDim.x);
+        wl = wc;
+        if (nmine > 0) load_patch(wl.box(g), sP);
+        else tc::cp_async_commit();
+        wl.next(g);
+        if (nmine > 1) load_patch(wl.box(g), sP + 3 * kPVol);
+        else tc::cp_async_commit();
+        wl.next(g);
+        for (int it = 0; it < nmine; ++it, wc.next(g), wl.next(g)) {
+            const int s = it & 1, pb = it % 3;
+            if (it + 2 < nmine) load_patch(wl.box(g), sP + ((it + 2) % 3) * 3 * kPVol);
             else tc::cp_async_commit();
-            const BrickBox bb = brick_box(g, b);
+            const BrickBox bb = wc.box(g);
             const bool fx = brick_needs(s_nonid[0], bb.x0, bb.ex_n, g.nx);
             const bool fy = brick_needs(s_nonid[1], bb.y0, bb.ey_n, g.ny);
             const bool fz = brick_needs(s_nonid[2], bb.z0, bb.ez_n, g.nz);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
-            tc::cp_async_wait<1>();
+            tc::cp_async_wait<2>();
             tc::named_sync(1, kRoleThreads);   // brick it's patch has landed for every builder
             if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
-            const float *Pc = sP + s * 3 * kPVol + base;
+            const float *Pc = sP + pb * 3 * kPVol + base;
             float v[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) v[a] = Pc[(a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
@@ -275,15 +324,20 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             if (fx) xform_dir<0, true>(v, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
             if (fy) xform_dir<1, true>(v, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
             if (fz) xform_dir<2, true>(v, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
+            // A_hi into TMEM (lane = element), A_lo into shared memory in the canonical layout
             const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(s * kColSlot + c * 32);
+            float *alo = sAlo + s * kAloFl + canon(q * 32 + lane, c * 32, kTcM);
 #pragma unroll
             for (int q8 = 0; q8 < 4; ++q8) {
                 float hi[8], lo[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) tc::split_tf32(q8 * 8 + j < 27 ? v[q8 * 8 + j] : 0.f, hi[j], lo[j]);
                 tc::tmem_st8(col + q8 * 8, hi);
-                tc::tmem_st8(col + kTcK + q8 * 8, lo);
+                // 4 consecutive k of one row are 16 contiguous bytes; k + 4 is one core-matrix column on
+                *reinterpret_cast<float4 *>(alo + (2 * q8) * (kTcM / 8) * 32) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+                *reinterpret_cast<float4 *>(alo + (2 * q8 + 1) * (kTcM / 8) * 32) = make_float4(lo[4], lo[5], lo[6], lo[7]);
             }
+            tc::fence_proxy_async();   // A_lo (generic-proxy stores) -> visible to the tensor core
             tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(&a_full[s]);
@@ -299,26 +353,31 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         const int c = (warp - kRoleWarps) >> 2, q = warp & 3;
         const int r = q * 32 + lane;
         const int lx = lane & 7, ly = lane >> 3;
-        const uint32_t dcol = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kColD + c * 32);
+        const uint32_t dcol0 = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kColD + c * 32);
         const unsigned FULL = 0xffffffffu;
-        float se_next = nmine > 0 ? row_scale(g, blockIdx.x, r, scale) : 0.f;
-        for (int it = 0; it < nmine; ++it) {
+        BrickWalk we;
+        we.init(g, blockIdx.x, gridDim.x);
+        BrickWalk wn = we;
+        wn.next(g);
+        float se_next = nmine > 0 ? row_scale(g, we.box(g), r, scale) : 0.f;
+        for (int it = 0; it < nmine; ++it, we.next(g), wn.next(g)) {
             const int b = blockIdx.x + it * gridDim.x;
             const float se = se_next;
             float *sZ = sZb + (it & 1) * kZFl;
-            const BrickBox bb = brick_box(g, b);
+            const BrickBox bb = we.box(g);
             const bool fx = brick_needs(s_nonid[0], bb.x0, bb.ex_n, g.nx);
             const bool fy = brick_needs(s_nonid[1], bb.y0, bb.ey_n, g.ny);
             const bool fz = brick_needs(s_nonid[2], bb.z0, bb.ez_n, g.nz);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
-            pt_wait(d_full, uint32_t(it) & 1u, &s_abort, err);
+            const int db = it & 1;
+            pt_wait(&d_full[db], uint32_t(it >> 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
             uint32_t dv[32];
-            tc::tmem_ld32(dcol, dv);
+            tc::tmem_ld32(dcol0 + (uint32_t)(db * kTcN), dv);
             tc::tmem_wait_ld();
             tc::fence_before_sync();
-            tc::mbar_arrive(d_empty);   // the accumulator is free for the next brick
-            if (it + 1 < nmine) se_next = row_scale(g, b + gridDim.x, r, scale);
+            tc::mbar_arrive(&d_empty[db]);   // accumulator buffer db is free for brick it + 2
+            if (it + 1 < nmine) se_next = row_scale(g, wn.box(g), r, scale);
             float res[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
@@ -387,27 +446,31 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         // descriptors of K step 0 (hi and lo terms); the shared-memory window is below 256 KB,
         // so adding a step's offset never carries out of the address field
         const uint64_t dbh0 = tc::make_desc(sB, kBLbo, kSbo), dbl0 = tc::make_desc(sB + kBFl, kBLbo, kSbo);
+        const uint64_t dal0 = tc::make_desc(sAlo, kALbo, kSbo), dal1 = tc::make_desc(sAlo + kAloFl, kALbo, kSbo);
         for (int it = 0; it < nmine; ++it) {
-            const int s = it & 1;
+            const int s = it & 1, db = it & 1;
             pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
-            // the previous brick has been drained: no MMA still writes the accumulator
-            if (it >= 1) pt_wait(d_empty, uint32_t(it - 1) & 1u, &s_abort, err);
+            // brick it - 2 has been drained from accumulator buffer db
+            if (it >= 2) pt_wait(&d_empty[db], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
             const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
+            const uint32_t dacc = tmem + (uint32_t)(kColD + db * kTcN);
+            const uint64_t dal = s ? dal1 : dal0;
 #pragma unroll
             for (int ks = 0; ks < kTcKSteps; ++ks) {
-                // one K step of 8 = two core-matrix columns: advance the start address field
-                const uint64_t dk = (uint64_t)(ks * 2 * kBLbo) >> 4;
+                // one K step of 8 = two core-matrix columns: advance the start address fields
+                const uint64_t dk = (uint64_t)(ks * 2 * kBLbo) >> 4, dka = (uint64_t)(ks * 2 * kALbo) >> 4;
                 const uint64_t dbh = dbh0 + dk, dbl = dbl0 + dk;
-                const uint32_t ah = acol + ks * 8, al = acol + kTcK + ks * 8;
-                tc::mma_tf32_ts(tmem + kColD, al, dbh, idesc, ks > 0 ? 1u : 0u);
-                tc::mma_tf32_ts(tmem + kColD, ah, dbl, idesc, 1u);
-                tc::mma_tf32_ts(tmem + kColD, ah, dbh, idesc, 1u);
+                const uint32_t ah = acol + ks * 8;
+                tc::mma_tf32(dacc, dal + dka, dbh, idesc, ks > 0 ? 1u : 0u);   // A_lo B_hi
+                tc::mma_tf32_ts(dacc, ah, dbl, idesc, 1u);                     // A_hi B_lo
+                tc::mma_tf32_ts(dacc, ah, dbh, idesc, 1u);                     // A_hi B_hi
             }
-            tc::mma_commit(d_full);
+            tc::mma_commit(&d_full[db]);
             tc::mma_commit(&a_empty[s]);
         }
-        if (nmine >= 1) pt_wait(d_empty, uint32_t(nmine - 1) & 1u, &s_abort, err);
+        for (int it = nmine - 2; it < nmine; ++it)
+            if (it >= 0) pt_wait(&d_empty[it & 1], uint32_t(it >> 1) & 1u, &s_abort, err);
     }
     tc::fence_before_sync();
     __syncthreads();
