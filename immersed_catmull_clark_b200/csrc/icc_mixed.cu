@@ -68,6 +68,7 @@ struct MixedState {
     bool ready = false;
     float4 *d_bmat = nullptr;        // K_main split [hi, lo][kBFl] in the canonical layout
     Xform xf{};
+    uint8_t *d_bflags = nullptr;     // per brick: bit d set when an element needs R along direction d
     float *d_scale32 = nullptr;
     float *d_patch32 = nullptr;
     float *d_rhs32 = nullptr, *d_x32 = nullptr, *d_r32 = nullptr, *d_p32 = nullptr, *d_ap32 = nullptr,
@@ -210,9 +211,12 @@ __device__ __forceinline__ float row_scale(const Geom &g, const BrickBox &bb, in
     return 0.f;
 }
 
+// 25 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
+// the compiler caps a thread at 72
 __global__ void __launch_bounds__(kPtThreads, 1)
 apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ scale, const float4 *__restrict__ bmat,
-                const Xform xf, float *__restrict__ patch_out, int *__restrict__ err, const PcgState *__restrict__ st) {
+                const Xform xf, const uint8_t *__restrict__ bflags, float *__restrict__ patch_out, int *__restrict__ err,
+                const PcgState *__restrict__ st) {
     if (st && st->status != 0) return;
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
@@ -296,15 +300,16 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         if (nmine > 1) load_patch(wl.box(g), sP + 3 * kPVol);
         else tc::cp_async_commit();
         wl.next(g);
+        unsigned fl_next = nmine > 0 ? bflags[blockIdx.x] : 0u;
         for (int it = 0; it < nmine; ++it, wc.next(g), wl.next(g)) {
             const int s = it & 1, pb = it % 3;
+            const unsigned fl = fl_next;   // bit d: the brick needs R along direction d
+            if (it + 1 < nmine) fl_next = bflags[blockIdx.x + (it + 1) * gridDim.x];
             if (it + 2 < nmine) load_patch(wl.box(g), sP + ((it + 2) % 3) * 3 * kPVol);
             else tc::cp_async_commit();
             const BrickBox bb = wc.box(g);
-            const bool fx = brick_needs(s_nonid[0], bb.x0, bb.ex_n, g.nx);
-            const bool fy = brick_needs(s_nonid[1], bb.y0, bb.ey_n, g.ny);
-            const bool fz = brick_needs(s_nonid[2], bb.z0, bb.ez_n, g.nz);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
+            const float vm = valid ? 1.f : 0.f;
             tc::cp_async_wait<2>();
             tc::named_sync(1, kRoleThreads);   // brick it's patch has landed for every builder
             if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
@@ -318,12 +323,12 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             // split operands carry only the variation across the element; the TF32 splitting
             // error then scales with that variation instead of with |u| (smooth, low-energy
             // vectors of a converging PCG).  R^T maps constants to themselves.
-            const float ctr = v[13];
+            const float nctr = -v[13] * vm;
 #pragma unroll
-            for (int a = 0; a < 27; ++a) v[a] = valid ? v[a] - ctr : 0.f;
-            if (fx) xform_dir<0, true>(v, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
-            if (fy) xform_dir<1, true>(v, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
-            if (fz) xform_dir<2, true>(v, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
+            for (int a = 0; a < 27; ++a) v[a] = fmaf(v[a], vm, nctr);   // (v - ctr), or 0 outside the grid
+            if (fl & 1u) xform_dir<0, true>(v, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
+            if (fl & 2u) xform_dir<1, true>(v, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
+            if (fl & 4u) xform_dir<2, true>(v, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
             // A_hi into TMEM (lane = element), A_lo into shared memory in the canonical layout
             const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(s * kColSlot + c * 32);
             float *alo = sAlo + s * kAloFl + canon(q * 32 + lane, c * 32, kTcM);
@@ -360,14 +365,27 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         BrickWalk wn = we;
         wn.next(g);
         float se_next = nmine > 0 ? row_scale(g, we.box(g), r, scale) : 0.f;
+        unsigned fl_next = nmine > 0 ? bflags[blockIdx.x] : 0u;
+        // lane masks of the node sums as multipliers (FMA instead of selects)
+        const float mx1 = lx >= 1 ? 1.f : 0.f, mx2 = lx >= 2 ? 1.f : 0.f;
+        const float my1 = ly >= 1 ? 1.f : 0.f, my2 = ly >= 2 ? 1.f : 0.f;
+        // z-sum: this thread's outputs i = et + k * 384 of the brick; the term of layer lz = pz - az
+        // sits at sZ[((lz * 3 + az) * 3 + ci) * 60 + pyx] = sZ[zb - 360 az] with zb = 540 pz + 60 ci + pyx
+        int zb[3], zpz[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int i = et + k * kRoleThreads;
+            const int ci = i / kPVol, rem = i - ci * kPVol;
+            const int pz = rem / (kPX * kPY), pyx = rem - pz * (kPX * kPY);
+            zb[k] = 9 * (kPY * kPX) * pz + (kPY * kPX) * ci + pyx;
+            zpz[k] = pz;
+        }
         for (int it = 0; it < nmine; ++it, we.next(g), wn.next(g)) {
             const int b = blockIdx.x + it * gridDim.x;
             const float se = se_next;
+            const unsigned fl = fl_next;
             float *sZ = sZb + (it & 1) * kZFl;
             const BrickBox bb = we.box(g);
-            const bool fx = brick_needs(s_nonid[0], bb.x0, bb.ex_n, g.nx);
-            const bool fy = brick_needs(s_nonid[1], bb.y0, bb.ey_n, g.ny);
-            const bool fz = brick_needs(s_nonid[2], bb.z0, bb.ez_n, g.nz);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const int db = it & 1;
             pt_wait(&d_full[db], uint32_t(it >> 1) & 1u, &s_abort, err);
@@ -377,13 +395,16 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             tc::tmem_wait_ld();
             tc::fence_before_sync();
             tc::mbar_arrive(&d_empty[db]);   // accumulator buffer db is free for brick it + 2
-            if (it + 1 < nmine) se_next = row_scale(g, wn.box(g), r, scale);
+            if (it + 1 < nmine) {
+                se_next = row_scale(g, wn.box(g), r, scale);
+                fl_next = bflags[b + gridDim.x];
+            }
             float res[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
-            if (fx) xform_dir<0, false>(res, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
-            if (fy) xform_dir<1, false>(res, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
-            if (fz) xform_dir<2, false>(res, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
+            if (fl & 1u) xform_dir<0, false>(res, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
+            if (fl & 2u) xform_dir<1, false>(res, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
+            if (fl & 4u) xform_dir<2, false>(res, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] *= se;
             // x, in place: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2) in res[o]; lanes
@@ -396,8 +417,8 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
                     const float a0 = res[o], a1 = res[o + 1], a2 = res[o + 2];
                     const float u1 = __shfl_up_sync(FULL, a1, 1), u2 = __shfl_up_sync(FULL, a2, 2);
                     const float w1 = __shfl_up_sync(FULL, a2, 1);
-                    res[o] = (a0 + (lx >= 1 ? u1 : 0.f)) + (lx >= 2 ? u2 : 0.f);
-                    res[o + 1] = a1 + (lx >= 1 ? w1 : 0.f);
+                    res[o] = fmaf(mx2, u2, fmaf(mx1, u1, a0));   // (a0 + u1) + u2 on lanes that have them
+                    res[o + 1] = fmaf(mx1, w1, a1);
                 }
             // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also carry
             // py = 4 and py = 5.  Results are this layer's partials for z-offset az.
@@ -408,8 +429,8 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
                     const float a0 = res[9 * az + var], a1 = res[9 * az + 3 + var], a2 = res[9 * az + 6 + var];
                     const float s1 = __shfl_up_sync(FULL, a1, 8), s2 = __shfl_up_sync(FULL, a2, 16);
                     const float t1 = __shfl_up_sync(FULL, a2, 8);
-                    const float yv = (a0 + (ly >= 1 ? s1 : 0.f)) + (ly >= 2 ? s2 : 0.f);
-                    const float y4 = a1 + (ly >= 1 ? t1 : 0.f);
+                    const float yv = fmaf(my2, s2, fmaf(my1, s1, a0));
+                    const float y4 = fmaf(my1, t1, a1);
                     const int px = var == 0 ? lx : 7 + var;
                     if (var == 0 || lx == 7) {
                         float *zb = sZ + (((q * 3 + az) * 3 + c) * kPY) * kPX + px;
@@ -424,17 +445,15 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             // the other buffer) finished before its thread reached this barrier
             tc::named_sync(2, kRoleThreads);
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
-            float *ob = patch_out + (size_t)b * 3 * kPVol;
-            for (int i = et; i < 3 * kPVol; i += kRoleThreads) {
-                const int ci = i / kPVol, rem = i - ci * kPVol;
-                const int pz = rem / (kPX * kPY), pyx = rem - pz * (kPX * kPY);
+            float *ob = patch_out + (size_t)b * 3 * kPVol + et;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (et + k * kRoleThreads >= 3 * kPVol) break;
                 float sum = 0.f;
 #pragma unroll
-                for (int az = 0; az < 3; ++az) {
-                    const int lz = pz - az;
-                    if (lz >= 0 && lz < kBZ) sum += sZ[((lz * 3 + az) * 3 + ci) * (kPY * kPX) + pyx];
-                }
-                ob[i] = sum;
+                for (int az = 0; az < 3; ++az)
+                    if (zpz[k] - az >= 0 && zpz[k] - az < kBZ) sum += sZ[zb[k] - 2 * 3 * (kPY * kPX) * az];
+                ob[k * kRoleThreads] = sum;
             }
         }
     } else if (lane == 0) {
@@ -706,6 +725,18 @@ static int mixed_init(Op &op) {
     if ((rc = dalloc(&ms.d_bmat, bm.size() / 4, "alloc tc matrices"))) return rc;
     ICC_CUDA(cudaMemcpy(ms.d_bmat, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice), "copy tc matrices");
     const Geom &g = op.g;
+    {
+        std::vector<uint8_t> fl((size_t)g.nbricks, 0);
+        const int n[3] = {g.nx, g.ny, g.nz}, be[3] = {kBX, kBY, kBZ};
+        for (int b = 0; b < g.nbricks; ++b) {
+            const int bi[3] = {b % g.nbx, (b / g.nbx) % g.nby, b / (g.nbx * g.nby)};
+            for (int d = 0; d < 3; ++d)
+                for (int e = bi[d] * be[d]; e < std::min(n[d], (bi[d] + 1) * be[d]); ++e)
+                    if ((ms.xf.nonid[d] >> pos_class(e, n[d])) & 1u) fl[(size_t)b] |= uint8_t(1u << d);
+        }
+        if ((rc = dalloc(&ms.d_bflags, fl.size(), "alloc brick flags"))) return rc;
+        ICC_CUDA(cudaMemcpy(ms.d_bflags, fl.data(), fl.size(), cudaMemcpyHostToDevice), "copy brick flags");
+    }
     const size_t n = (size_t)op.ndof;
     if ((rc = dalloc(&ms.d_scale32, (size_t)op.nel, "alloc mixed"))) return rc;
     if ((rc = dalloc(&ms.d_patch32, (size_t)g.nbricks * 3 * kPVol, "alloc mixed"))) return rc;
@@ -731,7 +762,7 @@ void mixed_release(Op &op) {
     if (!op.mixed) return;
     MixedState &ms = *op.mixed;
     if (ms.graph) cudaGraphExecDestroy(ms.graph);
-    void *bufs[] = {ms.d_bmat, ms.d_scale32, ms.d_patch32, ms.d_rhs32, ms.d_x32, ms.d_r32, ms.d_p32,
+    void *bufs[] = {ms.d_bmat, ms.d_bflags, ms.d_scale32, ms.d_patch32, ms.d_rhs32, ms.d_x32, ms.d_r32, ms.d_p32,
                     ms.d_ap32, ms.d_inv32, ms.d_xm32, ms.d_x64, ms.d_r64, ms.d_y64, ms.d_scalars,
                     ms.d_err, ms.d_state};
     for (void *p : bufs)
@@ -761,7 +792,7 @@ static void launch_apply_tc(Op &op, const float *xin, const PcgState *st) {
     MixedState &ms = *op.mixed;
     const int grid = std::min(op.num_sms, op.g.nbricks);
     apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, ms.d_bmat, ms.xf,
-                                                              ms.d_patch32, ms.d_err, st);
+                                                              ms.d_bflags, ms.d_patch32, ms.d_err, st);
 }
 
 // enqueue y32 = A x32 with the tensor-core apply; a masked operator first zeroes the fixed DOFs of
