@@ -86,16 +86,18 @@ struct MixedState {
 // ------------------------------------------------------------------------------------------
 
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
-// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (13 warps):
-//   warps 0-3 (builders): prefetch the next brick's input patch with cp.async; per component,
-//     gather each element's 27 values, shift them by the element's centre value, apply R^T along
-//     the directions where the brick touches a boundary class, split into TF32 hi/lo and store
-//     them as the A operand straight into TMEM (row m = element m = lane m), in two A slots;
-//   warp 12 (MMA): holds B = K_main hi/lo in shared memory and issues the 36 tcgen05.mma (A from
-//     TMEM, B from shared memory) of a brick into the TMEM accumulator;
-//   warps 4-11 (epilogue, two groups of 4 taking alternate bricks): read the accumulator with
-//     tcgen05.ld and release it, apply R, scale by s_e and sum the element results per patch node
-//     with warp shuffles (x, y) and a small shared buffer (z), then write the brick partials.
+// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (25 warps):
+//   warps 0-11 (builders, warp 4 c + q: component c of z-layer q): fetch the input patch two
+//     bricks ahead with cp.async; gather each element's 27 values of component c, shift them by
+//     the element's centre value and scale by s_e, apply R^T along the directions where the brick
+//     touches a boundary class, split into TF32 hi/lo and store A_hi into TMEM (row m = element m
+//     = lane m) and A_lo into shared memory, in two A slots;
+//   warp 24 (MMA, one thread): holds B = K_main hi/lo in shared memory and issues the 36
+//     tcgen05.mma of a brick (A_lo B_hi from shared memory, A_hi B_lo and A_hi B_hi with A from
+//     TMEM) into one of two TMEM accumulators;
+//   warps 12-23 (epilogue, same split): read their 32 accumulator columns with tcgen05.ld and
+//     release them, apply R and sum the element results per patch node with warp shuffles (x, y)
+//     and a shared buffer (z), then write the brick partials.
 // mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full.
 // Every wait is bounded; on time-out the CTA raises a shared abort flag, so all roles finish
 // promptly and the host reports ICC_TIMEOUT.
@@ -301,15 +303,23 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         else tc::cp_async_commit();
         wl.next(g);
         unsigned fl_next = nmine > 0 ? bflags[blockIdx.x] : 0u;
+        const int r = q * 32 + lane;
+        float se_next = nmine > 0 ? row_scale(g, wc.box(g), r, scale) : 0.f;
         for (int it = 0; it < nmine; ++it, wc.next(g), wl.next(g)) {
             const int s = it & 1, pb = it % 3;
             const unsigned fl = fl_next;   // bit d: the brick needs R along direction d
-            if (it + 1 < nmine) fl_next = bflags[blockIdx.x + (it + 1) * gridDim.x];
+            const float se = se_next;      // s_e of this thread's element (0 outside the grid)
+            if (it + 1 < nmine) {
+                fl_next = bflags[blockIdx.x + (it + 1) * gridDim.x];
+                BrickWalk wn1 = wc;
+                wn1.next(g);
+                se_next = row_scale(g, wn1.box(g), r, scale);
+            }
             if (it + 2 < nmine) load_patch(wl.box(g), sP + ((it + 2) % 3) * 3 * kPVol);
             else tc::cp_async_commit();
             const BrickBox bb = wc.box(g);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
-            const float vm = valid ? 1.f : 0.f;
+            const float vm = valid ? se : 0.f;
             tc::cp_async_wait<2>();
             tc::named_sync(1, kRoleThreads);   // brick it's patch has landed for every builder
             if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
@@ -325,7 +335,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             // vectors of a converging PCG).  R^T maps constants to themselves.
             const float nctr = -v[13] * vm;
 #pragma unroll
-            for (int a = 0; a < 27; ++a) v[a] = fmaf(v[a], vm, nctr);   // (v - ctr), or 0 outside the grid
+            for (int a = 0; a < 27; ++a) v[a] = fmaf(v[a], vm, nctr);   // s_e (v - ctr), or 0 outside the grid
             if (fl & 1u) xform_dir<0, true>(v, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
             if (fl & 2u) xform_dir<1, true>(v, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
             if (fl & 4u) xform_dir<2, true>(v, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
@@ -364,7 +374,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         we.init(g, blockIdx.x, gridDim.x);
         BrickWalk wn = we;
         wn.next(g);
-        float se_next = nmine > 0 ? row_scale(g, we.box(g), r, scale) : 0.f;
         unsigned fl_next = nmine > 0 ? bflags[blockIdx.x] : 0u;
         // lane masks of the node sums as multipliers (FMA instead of selects)
         const float mx1 = lx >= 1 ? 1.f : 0.f, mx2 = lx >= 2 ? 1.f : 0.f;
@@ -382,7 +391,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         }
         for (int it = 0; it < nmine; ++it, we.next(g), wn.next(g)) {
             const int b = blockIdx.x + it * gridDim.x;
-            const float se = se_next;
             const unsigned fl = fl_next;
             float *sZ = sZb + (it & 1) * kZFl;
             const BrickBox bb = we.box(g);
@@ -395,18 +403,13 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             tc::tmem_wait_ld();
             tc::fence_before_sync();
             tc::mbar_arrive(&d_empty[db]);   // accumulator buffer db is free for brick it + 2
-            if (it + 1 < nmine) {
-                se_next = row_scale(g, wn.box(g), r, scale);
-                fl_next = bflags[b + gridDim.x];
-            }
+            if (it + 1 < nmine) fl_next = bflags[b + gridDim.x];
             float res[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
             if (fl & 1u) xform_dir<0, false>(res, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
             if (fl & 2u) xform_dir<1, false>(res, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
             if (fl & 4u) xform_dir<2, false>(res, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
-#pragma unroll
-            for (int a = 0; a < 27; ++a) res[a] *= se;
             // x, in place: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2) in res[o]; lanes
             // lx = 7 also carry px = 8 (v[1](7) + v[2](6)) in res[o+1] and px = 9 (v[2](7)) in res[o+2]
 #pragma unroll

@@ -76,32 +76,40 @@ gather_kernel(Geom g, const T *__restrict__ patch, const T *__restrict__ p, cons
               PcgState *fuse = nullptr, unsigned *counter = nullptr) {
     if (st && st->status != 0) return;
     double dot = 0.0;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
-         n += (long long)gridDim.x * blockDim.x) {
-        int ix = int(n % g.cx), iy = int((n / g.cx) % g.cy), iz = int(n / ((long long)g.cx * g.cy));
-        int bx[2], lx[2], by[2], ly[2], bz[2], lz[2];
-        int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
-        int nby = node_bricks(iy, kBY, g.nby, by, ly);
-        int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
-        T s0 = T(0), s1 = T(0), s2 = T(0);
-        for (int a = 0; a < nbz; ++a)
-            for (int q = 0; q < nby; ++q)
-                for (int w = 0; w < nbx; ++w) {
-                    size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
-                    const T *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
-                    s0 += pb[0];
-                    s1 += pb[kPVol];
-                    s2 += pb[2 * kPVol];
-                }
-        T sv[3] = {s0, s1, s2};
+    // one warp per row (iy, iz) of control points, lanes along x: the brick partials of
+    // neighbouring nodes are neighbouring floats, and the row's divisions are paid once
+    const int lane = threadIdx.x & 31;
+    const int nrows = g.cy * g.cz;
+    const int wstride = (gridDim.x * blockDim.x) >> 5;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nrows; row += wstride) {
+        const int iy = row % g.cy, iz = row / g.cy;
+        int by[2], ly[2], bz[2], lz[2];
+        const int nby = node_bricks(iy, kBY, g.nby, by, ly);
+        const int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
+        for (int ix = lane; ix < g.cx; ix += 32) {
+            const long long n = (long long)row * g.cx + ix;
+            int bx[2], lx[2];
+            const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
+            T s0 = T(0), s1 = T(0), s2 = T(0);
+            for (int a = 0; a < nbz; ++a)
+                for (int q = 0; q < nby; ++q)
+                    for (int w = 0; w < nbx; ++w) {
+                        size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
+                        const T *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
+                        s0 += pb[0];
+                        s1 += pb[kPVol];
+                        s2 += pb[2 * kPVol];
+                    }
+            T sv[3] = {s0, s1, s2};
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            long long idx = (long long)c * g.nsc + n;
-            T v = sv[c];
-            if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = T(0);
-            else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
-            y[idx] = v;
-            if (partials) dot += double(p[idx]) * double(v);
+            for (int c = 0; c < 3; ++c) {
+                long long idx = (long long)c * g.nsc + n;
+                T v = sv[c];
+                if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = T(0);
+                else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
+                y[idx] = v;
+                if (partials) dot += double(p[idx]) * double(v);
+            }
         }
     }
     if (partials) {
