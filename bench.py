@@ -4,15 +4,18 @@
 Workload (default): the SIMP cantilever on 128 x 64 x 64 elements (1,698,840 DOF), box
 [0,2]x[0,1]x[0,1], densities i.i.d. U[0.01,1] smoothed by a 3x3x3 box filter (seeded PCG64),
 E0 = 1, E_min = 1e-9, nu = 0.3, SIMP penalty 3, x = 0 clamped, unit downward traction on x = 2.
-One step = one Jacobi-PCG solve to relative residual 1e-8 from x = 0.
+One step = one Jacobi-PCG solve to relative residual 1e-8 from x = 0, in the mixed-precision form
+(tensor-core split-TF32 FP32 iterations with FP64 residual replacement) by default; the plain FP64
+solve of the same system is timed beside it (config.vs_fp64).  --mode fp64 times the plain solve only.
 
 value    = DOF * iterations / device seconds of the solve, inputs resident in HBM (CUDA events on
            the solver's stream, L2 flushed between steps), summed over ranks (replicas).
 e2e      = the same metric through the host-pointer C ABI call (icc_op_update_scale +
            icc_pcg_solve): H2D of the step's scale and load, D2H of the solution, inside the timing.
-roofline = the FP64 brick contraction kernel: algorithmic 2*81*81 flops per element per launch
-           over its mean CUDA-event duration, against this run's measured FP64 DMMA peak
-           (cuBLAS DGEMM through torch.matmul on float64, 8192^3).
+roofline = the dominant kernel: for the mixed form the tensor-core brick apply, algorithmic
+           3 * 2*81*81 flops per element (three split-TF32 products) over its mean CUDA-event
+           duration against this run's cuBLAS TF32 GEMM; for --mode fp64 the FP64 DMMA brick apply,
+           2*81*81 flops per element against this run's cuBLAS DGEMM.
 cpu_baseline / --impl reference = the oracle (C restatement of the reference's CPU path:
            element-loop operator with OpenMP, serial PCG vector loops) on the host cores, a
            bounded number of PCG iterations of the same workload.
@@ -48,7 +51,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cantilever128", choices=sorted(WORKLOADS))
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mode", default="mixed", choices=["fp64", "mixed"],
+                    help="mixed: the tensor-core solve, timed beside the plain FP64 solve; fp64: the plain solve only")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-solution", action="store_true", help="skip the tight FP64 error reference")
@@ -122,11 +126,14 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def fp64_tensor_peak(torch, dev):
-    """Measured FP64 tensor-core peak of this GPU: cuBLAS DGEMM (torch.matmul float64), TFLOP/s."""
+def gemm_peak(torch, dev, dtype, tf32=False):
+    """Measured tensor-core peak of this GPU for one GEMM type: cuBLAS through torch.matmul, 8192^3,
+    best of 5 (TFLOP/s).  float64 -> DGEMM; float32 with tf32=True -> TF32 tensor cores."""
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device=dev)
-    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = tf32
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
     for _ in range(2):
         torch.matmul(a, b)
     torch.cuda.synchronize()
@@ -138,6 +145,7 @@ def fp64_tensor_peak(torch, dev):
         e1.record()
         e1.synchronize()
         best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = old
     del a, b
     torch.cuda.empty_cache()
     return best
@@ -247,45 +255,71 @@ def run_ours(args):
                               "ms_per_apply": e0.elapsed_time(e1) / args.steps}), flush=True)
         return
 
-    for _ in range(args.warmup):
-        solver.solve_dev(n, b_dev.data_ptr(), 0, x_dev.data_ptr(), op)
-    barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    iters, launches = [], 0
-    with ClockSampler(torch.cuda.current_device()) as clk:
+    def timed_solves(slv, steps, warmup, x_out):
+        for _ in range(warmup):
+            slv.solve_dev(n, b_dev.data_ptr(), 0, x_out.data_ptr(), op)
         barrier()
-        for i in range(args.steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        iters, launches = [], 0
+        for i in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 ev[i][0].record(stream)
-            it, res = solver.solve_dev(n, b_dev.data_ptr(), 0, x_dev.data_ptr(), op)
+            it, res = slv.solve_dev(n, b_dev.data_ptr(), 0, x_out.data_ptr(), op)
             with torch.cuda.stream(stream):
                 ev[i][1].record(stream)
-            iters.append(it)
+            iters.append(int(it))
             launches += op.last_solve_info().kernel_launches
         barrier()
-    ms_steps = [a.elapsed_time(b) for a, b in ev]
+        return [a_.elapsed_time(b_) for a_, b_ in ev], iters, launches, op.last_solve_info()
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms_steps, iters, launches, info = timed_solves(solver, args.steps, args.warmup, x_dev)
     t_ms = float(np.sum(ms_steps))
     local_value = n * float(np.sum(iters)) / (t_ms * 1e-3)
-    info = op.last_solve_info()
 
-    # roofline of the dominant kernel (FP64 brick contraction), timed on the solver's stream
-    y_dev = torch.empty_like(x_dev)
-    p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev)
-    contract_ms, gather_ms = op.profile_apply(p_dev.data_ptr(), y_dev.data_ptr(), 20)
-    flops = 2.0 * 81 * 81 * sp.nel
+    # the plain FP64 solve of the same system, timed the same way, for the mixed/FP64 comparison
+    cmp = None
+    if precision == icc.MIXED:
+        x64_dev = torch.zeros_like(x_dev)
+        s64 = icc.PcgSolver(min(20 * n, 100000), TOL, precision=icc.FP64, check_every=args.check_every)
+        k64 = max(1, min(args.steps, 2))
+        ms64, it64, _, _ = timed_solves(s64, k64, 1, x64_dev)
+        t_mixed, t_fp64 = float(np.mean(ms_steps)), float(np.mean(ms64))
+        cmp = {"fp64_time_to_tol_ms": t_fp64, "fp64_iterations": it64, "mixed_time_to_tol_ms": t_mixed,
+               "mixed_iterations": iters, "speedup_time_to_tol": t_fp64 / t_mixed}
+
+    # roofline of the dominant kernel, timed on the solver's stream
+    flops_el = 2.0 * 81 * 81
+    if precision == icc.MIXED:
+        y32 = torch.empty(n, dtype=torch.float32, device=dev)
+        p32 = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev).to(torch.float32)
+        contract_ms, gather_ms = op.profile_apply_f32(p32.data_ptr(), y32.data_ptr(), 20)
+        flops = 3.0 * flops_el * sp.nel   # the three split-TF32 products of every element
+        peak = gemm_peak(torch, dev, torch.float32, tf32=True)
+        kname, tkey = "apply_tc_kernel (tcgen05 kind::tf32, 3-term split)", "apply_tc_kernel"
+        peak_src = ("measured in this run: cuBLAS TF32 GEMM (torch.matmul float32 with TF32 tensor cores, 8192^3); "
+                    "MEASURED_PEAKS.json has no TF32 figure")
+    else:
+        y_dev = torch.empty_like(x_dev)
+        p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev)
+        contract_ms, gather_ms = op.profile_apply(p_dev.data_ptr(), y_dev.data_ptr(), 20)
+        flops = flops_el * sp.nel
+        peak = gemm_peak(torch, dev, torch.float64)
+        kname, tkey = "apply_f64_kernel (FP64 DMMA)", "apply_f64_kernel"
+        peak_src = ("measured in this run: cuBLAS DGEMM (torch.matmul float64 8192^3); "
+                    "MEASURED_PEAKS.json has no FP64 figure")
     achieved = flops / (contract_ms * 1e-3) / 1e12
-    peak = fp64_tensor_peak(torch, dev)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         try:
-            t = json.load(open(tpath)).get("apply_f64_kernel", {}).get(args.workload)
+            t = json.load(open(tpath)).get(tkey, {}).get(args.workload)
             traffic = None if t is None else float(t)
         except Exception:
             traffic = None
 
-    # end to end through the host-pointer C ABI (pinned host buffers)
+    # end to end through the host-pointer C ABI call (pinned host buffers)
     b_pin = torch.from_numpy(b_host).pin_memory()
     s_pin = torch.from_numpy(prob.scale.copy()).pin_memory()
     x_pin = torch.empty(n, dtype=torch.float64).pin_memory()
@@ -335,20 +369,20 @@ def run_ours(args):
         cpu.pop("seconds", None)
 
     if rank == 0:
+        cfg = {"workload": f"{prob.name} SIMP cantilever, smoothed densities" if wl["smooth"] else prob.name,
+               "ndof": n, "nel": sp.nel, "tol": TOL, "seed": SEED, "mode": args.mode,
+               "iterations": iters, "time_to_tol_ms": ms_steps,
+               "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
+        if cmp:
+            cfg["vs_fp64"] = cmp
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": t_ms_all / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == icc.FP64 else "tf32x3+f32+f64",
-               "data": "synthetic",
-               "config": {"workload": f"{prob.name} SIMP cantilever, smoothed densities" if wl["smooth"] else prob.name,
-                          "ndof": n, "nel": sp.nel, "tol": TOL, "seed": SEED, "mode": args.mode,
-                          "iterations": iters, "time_to_tol_ms": ms_steps,
-                          "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
-               "roofline": {"bound": "tensor", "kernel": "apply_f64_kernel (FP64 DMMA)", "achieved": achieved,
-                            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+               "data": "synthetic", "config": cfg,
+               "roofline": {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak,
+                            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                             "algorithmic_flops_per_launch": flops, "launch_ms": contract_ms,
-                            "node_sum_kernel_ms": gather_ms,
-                            "peak_source": "measured in this run: cuBLAS DGEMM (torch.matmul float64 8192^3), "
-                                           "FP64 is absent from MEASURED_PEAKS.json"},
+                            "node_sum_kernel_ms": gather_ms, "peak_source": peak_src},
                "cpu_baseline": cpu,
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n + 8 * sp.nel,
                        "d2h_bytes_per_step": 8 * n},

@@ -43,6 +43,7 @@ EXPORTED = [
     "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_apply_f32",
     "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
+    "icc_op_profile_apply_f32",
     "icc_apply_f64_noalloc",
 ]
 
@@ -107,6 +108,7 @@ def lib():
                                     C.POINTER(i64), C.POINTER(dbl)]
     L.icc_op_last_solve_info.argtypes = [vp, C.POINTER(SolveInfo)]
     L.icc_op_profile_apply.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
+    L.icc_op_profile_apply_f32.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.icc_apply_f64_noalloc.argtypes = [i64p, vp, i32, vp, vp, vp, vp, vp]
     _lib = L
     return L
@@ -243,6 +245,13 @@ class MatrixFreeOperator:
         a, g = C.c_double(), C.c_double()
         _check(lib().icc_op_profile_apply(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), reps, C.byref(a),
                                           C.byref(g)))
+        return a.value, g.value
+
+    def profile_apply_f32(self, x_ptr, y_ptr, reps=20):
+        """Mean device ms of (tensor-core brick kernel, node-sum kernel) over reps FP32 applies."""
+        a, g = C.c_double(), C.c_double()
+        _check(lib().icc_op_profile_apply_f32(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), reps, C.byref(a),
+                                              C.byref(g)))
         return a.value, g.value
 
     def last_solve_info(self):

@@ -844,6 +844,40 @@ int mixed_apply_f32(Op &op, const float *x, float *y) {
     return ICC_OK;
 }
 
+// Mean device ms of the brick kernel and of the node-side pass over `reps` FP32 applies.
+int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms) {
+    int rc = mixed_init(op);
+    if (rc) return rc;
+    MixedState &ms = *op.mixed;
+    std::vector<cudaEvent_t> ev(3 * size_t(reps));
+    for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(ev[3 * r], op.stream);
+        launch_apply_tc(op, x, nullptr);
+        cudaEventRecord(ev[3 * r + 1], op.stream);
+        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, x, op.d_mask,
+                                                                           ICC_MASK_NONE, y, nullptr, nullptr);
+        cudaEventRecord(ev[3 * r + 2], op.stream);
+    }
+    cudaError_t e = cudaEventSynchronize(ev.back());
+    double a = 0.0, gt = 0.0;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        float t1 = 0.f, t2 = 0.f;
+        cudaEventElapsedTime(&t1, ev[3 * r], ev[3 * r + 1]);
+        cudaEventElapsedTime(&t2, ev[3 * r + 1], ev[3 * r + 2]);
+        a += t1;
+        gt += t2;
+    }
+    for (auto &x2 : ev) cudaEventDestroy(x2);
+    ICC_CUDA(e, "profile tc apply");
+    int err = 0;
+    ICC_CUDA(cudaMemcpy(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
+    *contract_ms = a / reps;
+    *gather_ms = gt / reps;
+    return ICC_OK;
+}
+
 // x64 += sigma * xs32; xs32 = 0
 __global__ void ru_accumulate_kernel(long long n, double *__restrict__ x, float *__restrict__ xs, double sigma) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {

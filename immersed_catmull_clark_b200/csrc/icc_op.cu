@@ -697,6 +697,14 @@ int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t
     return ICC_OK;
 }
 
+int icc_op_profile_apply_f32(icc_op *op, const float *x_dev, float *y_dev, int32_t reps, double *contract_ms,
+                             double *gather_ms) {
+    if (!op || !x_dev || !y_dev || reps <= 0 || !contract_ms || !gather_ms)
+        return set_error(ICC_BAD_ARG, "icc_op_profile_apply_f32: bad argument");
+    cudaSetDevice(op->op.device);
+    return icc::mixed_profile_apply(op->op, x_dev, y_dev, reps, contract_ms, gather_ms);
+}
+
 int icc_op_last_solve_info(const icc_op *op, icc_solve_info *info) {
     if (!op || !info) return set_error(ICC_BAD_ARG, "icc_op_last_solve_info: null argument");
     *info = op->op.last_info;

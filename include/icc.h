@@ -153,6 +153,10 @@ int icc_apply_f64_noalloc(const int64_t nel_dir[3], const double *ke_types_dev, 
 int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t reps, double *contract_ms,
                          double *gather_ms);
 
+/* The same for the tensor-core FP32 apply (unmasked input x_dev, FP32 device arrays). */
+int icc_op_profile_apply_f32(icc_op *op, const float *x_dev, float *y_dev, int32_t reps, double *contract_ms,
+                             double *gather_ms);
+
 #ifdef __cplusplus
 }
 #endif
