@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-solution", action="store_true", help="skip the tight FP64 error reference")
+    ap.add_argument("--solves-only", action="store_true",
+                    help="only run the warmup + timed solves of the chosen mode (for profiler launch lists)")
     ap.add_argument("--kernel-only", action="store_true",
                     help="only run warmup + steps operator applies (for profiler captures)")
     ap.add_argument("--delta", type=float, default=0.0,
@@ -275,6 +277,11 @@ def run_ours(args):
 
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms_steps, iters, launches, info = timed_solves(solver, args.steps, args.warmup, x_dev)
+    if args.solves_only:
+        if rank == 0:
+            print(json.dumps({"solves_only": True, "workload": prob.name, "mode": args.mode, "iterations": iters,
+                              "time_to_tol_ms": ms_steps}), flush=True)
+        return
     t_ms = float(np.sum(ms_steps))
     local_value = n * float(np.sum(iters)) / (t_ms * 1e-3)
 
