@@ -31,6 +31,7 @@ constexpr int kStatConverged = 1;
 constexpr int kStatBreakdown = 2;
 constexpr int kStatMaxIter = 3;
 constexpr int kStatNan = 4;
+constexpr int kStatReplace = 5;   // mixed form: the FP32 recurrence wants an FP64 residual replacement
 
 struct Geom {
     int nx, ny, nz;        // elements per direction
@@ -45,6 +46,11 @@ struct PcgState {
     double rz_prev;        // r'z used by the last alpha (the beta of a residual replacement needs it)
     long long iter, max_iter;
     int status, pad;
+    // mixed form: ask for a residual replacement once rel_res < repl_delta * repl_res or after
+    // repl_seg iterations since iteration repl_iter (repl_delta = 0: never); the test runs every
+    // repl_every iterations (the host's batch), which keeps replacements from coming too often
+    double repl_res, repl_delta;
+    long long repl_iter, repl_seg, repl_every;   // tested only when iter is a multiple of repl_every
 };
 
 struct MixedState;  // tensor-core path (icc_mixed.cu)

@@ -206,6 +206,11 @@ pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, dou
         st->status = max_iter > 0 ? 0 : kStatMaxIter;
         st->alpha = st->beta = st->p_ap = 0.0;
         st->rz_prev = rz;
+        st->repl_res = 1.0;
+        st->repl_delta = 0.0;
+        st->repl_iter = 0;
+        st->repl_seg = 0;
+        st->repl_every = 1;
     }
 }
 

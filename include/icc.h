@@ -41,8 +41,10 @@ extern "C" {
 
 /* ---- precision forms of the solve ---------------------------------------------------------- */
 #define ICC_FP64 0            /* all-FP64 apply, vectors and reductions */
-#define ICC_MIXED 1           /* FP64 iterative refinement around an inner FP32 PCG whose apply runs
-                                 on the tensor cores as a 3-term split-TF32 product */
+#define ICC_MIXED 1           /* Jacobi-PCG whose iterations run in FP32 on the tensor-core apply (a
+                                 3-term split-TF32 product) with FP64 reductions, an FP64 solution and
+                                 FP64 residual replacement (reliable updates); stops on the FP64 true
+                                 residual */
 
 typedef struct icc_space icc_space;
 typedef struct icc_op icc_op;
@@ -50,14 +52,16 @@ typedef struct icc_op icc_op;
 typedef struct icc_solve_opts {
     int32_t precision;        /* ICC_FP64 or ICC_MIXED */
     int32_t check_every;      /* PCG iterations between convergence checks on the host (0: 32) */
-    double inner_tol;         /* ICC_MIXED: inner relative residual per refinement step (0: 1e-3) */
-    int32_t max_outer;        /* ICC_MIXED: maximum refinement steps (0: 60) */
+    double inner_tol;         /* ICC_MIXED: the FP32 residual is replaced by the FP64 true residual
+                                 whenever it has fallen by this factor since the last replacement
+                                 (0: 0.6) */
+    int32_t max_outer;        /* ICC_MIXED: maximum residual replacements (0: 1000) */
     int32_t reserved;
 } icc_solve_opts;
 
 typedef struct icc_solve_info {
     int64_t iterations;       /* PCG iterations (ICC_FP64) or inner iterations summed (ICC_MIXED) */
-    int64_t outer_iterations; /* refinement steps (ICC_MIXED), 0 otherwise */
+    int64_t outer_iterations; /* FP64 residual replacements (ICC_MIXED), 0 otherwise */
     double rel_res;           /* final relative residual (recurrence residual for ICC_FP64, as in
                                  rust/src/solver.rs:56-58; true FP64 residual for ICC_MIXED) */
     double device_ms;         /* device time of the solve (CUDA events on the handle's stream) */
