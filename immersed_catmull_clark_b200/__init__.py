@@ -43,7 +43,8 @@ EXPORTED = [
     "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_apply_f32",
     "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
-    "icc_op_profile_apply_f32",
+    "icc_op_profile_apply_f32", "icc_solve_state", "icc_op_element_energies", "icc_topopt_create",
+    "icc_topopt_destroy", "icc_topopt_run",
     "icc_apply_f64_noalloc",
 ]
 
@@ -63,6 +64,12 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int64), ("outer_iterations", C.c_int64), ("rel_res", C.c_double),
                 ("device_ms", C.c_double), ("fp64_applies", C.c_int64), ("mixed_applies", C.c_int64),
                 ("kernel_launches", C.c_int64)]
+
+
+class TopOptCfg(C.Structure):
+    _fields_ = [("size", C.c_double * 3), ("volfrac", C.c_double), ("penal", C.c_double), ("rmin", C.c_double),
+                ("young", C.c_double), ("poisson", C.c_double), ("emin", C.c_double), ("move_limit", C.c_double),
+                ("pcg_tol", C.c_double), ("precision", C.c_int32), ("reserved", C.c_int32)]
 
 
 _lib = None
@@ -110,6 +117,13 @@ def lib():
     L.icc_op_profile_apply.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.icc_op_profile_apply_f32.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.icc_apply_f64_noalloc.argtypes = [i64p, vp, i32, vp, vp, vp, vp, vp]
+    L.icc_solve_state.argtypes = [vp, f64p, f64p, i64, dbl, C.POINTER(SolveOpts), f64p, C.POINTER(i64),
+                                  C.POINTER(dbl)]
+    L.icc_op_element_energies.argtypes = [vp, f64p, i64, f64p, i64]
+    L.icc_topopt_create.argtypes = [i64p, C.POINTER(TopOptCfg), C.POINTER(vp)]
+    L.icc_topopt_destroy.argtypes = [vp]
+    L.icc_topopt_destroy.restype = None
+    L.icc_topopt_run.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(i32)]
     _lib = L
     return L
 
@@ -254,6 +268,13 @@ class MatrixFreeOperator:
                                               C.byref(g)))
         return a.value, g.value
 
+    def element_energies(self, u):
+        """u_e^T K_type(e) u_e per element (rust/src/topopt_iga.rs:165-184)."""
+        ee = np.zeros(self.sp.nel)
+        _check(lib().icc_op_element_energies(self._h, np.ascontiguousarray(u, dtype=np.float64), self.n, ee,
+                                             self.sp.nel))
+        return ee
+
     def last_solve_info(self):
         info = SolveInfo()
         _check(lib().icc_op_last_solve_info(self._h, C.byref(info)))
@@ -306,3 +327,53 @@ def apply_f64_noalloc(nel_dir, ke_ptr, ntypes, type_id_ptr, scale_ptr, x_ptr, y_
     _check(lib().icc_apply_f64_noalloc(ne, C.c_void_p(ke_ptr), int(ntypes), C.c_void_p(type_id_ptr),
                                        C.c_void_p(scale_ptr) if scale_ptr else None, C.c_void_p(x_ptr),
                                        C.c_void_p(y_ptr), C.c_void_p(stream) if stream else None))
+
+
+def solve_state(op, force, u0, pcg_tol, precision=FP64):
+    """Warm-started masked state solve (rust/src/topopt_iga.rs:137-162) on the device operator.
+    Returns (u, iterations, relative residual) as the reference does."""
+    u = np.zeros(op.n)
+    it, res = C.c_int64(), C.c_double()
+    opts = SolveOpts(precision, 32, 0.0, 0, 0)
+    rc = lib().icc_solve_state(op._h, np.ascontiguousarray(force, dtype=np.float64),
+                               np.ascontiguousarray(u0, dtype=np.float64), op.n, pcg_tol, C.byref(opts), u,
+                               C.byref(it), C.byref(res))
+    _check(rc, allow=(ICC_OK, ICC_NOT_CONVERGED, ICC_BREAKDOWN))
+    return u, it.value, res.value
+
+
+@dataclass
+class TopOptHistory:
+    """rust/src/topopt_iga.rs:53-58."""
+    compliance: np.ndarray
+    change: np.ndarray
+    pcg_iterations: np.ndarray
+    density: np.ndarray
+
+
+class CantileverTopOpt:
+    """SIMP cantilever loop on the device (rust/src/topopt_iga.rs:60-234, CantileverTopOptConfig
+    defaults)."""
+
+    def __init__(self, nel, size=(1.2, 0.6, 0.3), volfrac=0.3, penal=3.0, rmin=1.5, young=1.0, poisson=0.3,
+                 emin=1e-3, move_limit=0.2, pcg_tol=1e-10, precision=FP64):
+        cfg = TopOptCfg((C.c_double * 3)(*size), volfrac, penal, rmin, young, poisson, emin, move_limit, pcg_tol,
+                        precision, 0)
+        h = C.c_void_p()
+        _check(lib().icc_topopt_create(np.ascontiguousarray(nel, dtype=np.int64), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.nel = int(np.prod(nel))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.icc_topopt_destroy(h)
+            self._h = None
+
+    def run(self, max_iter=40):
+        comp, chg = np.zeros(max_iter), np.zeros(max_iter)
+        its, dens = np.zeros(max_iter, dtype=np.int64), np.zeros(self.nel)
+        done = C.c_int32()
+        _check(lib().icc_topopt_run(self._h, max_iter, _vp(comp), _vp(chg), _vp(its), _vp(dens), C.byref(done)))
+        k = done.value
+        return TopOptHistory(comp[:k], chg[:k], its[:k], dens)

@@ -54,6 +54,7 @@ struct PcgState {
 };
 
 struct MixedState;  // tensor-core path (icc_mixed.cu)
+struct StateScratch;  // warm-started state solve and element energies (icc_topopt.cu)
 
 struct Op {
     int device = 0, num_sms = 148, vec_blocks = 592;
@@ -83,11 +84,13 @@ struct Op {
     std::vector<int> host_type1d[3];                     // 1-D type of every element position
     std::vector<std::array<double, 9>> host_basis1d[3];  // basis values per 1-D type (Space::basis1d)
     MixedState *mixed = nullptr;
+    StateScratch *state = nullptr;
 
     ~Op();
     int init(const Space &s, const double *ke_types, int nt, const int32_t *type_id, const double *scale,
              const uint8_t *free_mask, int mode);
     int set_scale(const double *scale);
+    int set_scale_dev(const double *scale_dev);   // device array, stream-ordered
     int set_mask(const uint8_t *free_mask, int mode);
     void enqueue_apply(const double *x, double *y, double *partials, const PcgState *st);
     int apply_dev(const double *x, double *y);
@@ -102,6 +105,7 @@ int cuda_fail(cudaError_t e, const char *where);
 
 // tensor-core mixed-precision path (icc_mixed.cu)
 void mixed_release(Op &op);
+void state_release(Op &op);
 int mixed_on_scale_update(Op &op);
 int mixed_apply_f32(Op &op, const float *x, float *y);
 int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms);
@@ -141,3 +145,13 @@ __device__ __forceinline__ double block_sum(double v) {
 }
 
 }  // namespace icc
+
+// The C-ABI operator handle.
+struct icc_op {
+    icc::Op op;
+};
+
+// Solve on device arrays with the handle's operator (icc_pcg_solve_dev without the final sync);
+// internal, not part of include/icc.h.
+extern "C" int icc_solve_common(icc_op *op, const double *b_dev, const double *diag_dev, int64_t n, double tol,
+                     int64_t max_iter, const icc_solve_opts *opts, double *x_dev, int64_t *iters, double *rel_res);

@@ -133,18 +133,6 @@ struct BrickBox {
     int x0, y0, z0, ex_n, ey_n, ez_n;
 };
 
-__device__ __forceinline__ BrickBox brick_box(const Geom &g, int b) {
-    BrickBox r;
-    const int bxi = b % g.nbx, byi = (b / g.nbx) % g.nby, bzi = b / (g.nbx * g.nby);
-    r.x0 = bxi * kBX;
-    r.y0 = byi * kBY;
-    r.z0 = bzi * kBZ;
-    r.ex_n = min(kBX, g.nx - r.x0);
-    r.ey_n = min(kBY, g.ny - r.y0);
-    r.ez_n = min(kBZ, g.nz - r.z0);
-    return r;
-}
-
 // Walks the bricks b, b + step, b + 2 step, ... of a persistent CTA without integer divisions in
 // the loop (the step is split into per-direction increments once).
 struct BrickWalk {
@@ -177,19 +165,6 @@ struct BrickWalk {
         return r;
     }
 };
-
-// does any element of the brick along one direction (positions e0 .. e0 + cnt - 1) need R?
-// Only the interior class (positions 2 .. n-3) and the positions 0, 1, n-2, n-1 can differ.
-__device__ __forceinline__ bool brick_needs(unsigned nonid, int e0, int cnt, int n) {
-    const int e1 = e0 + cnt - 1;
-    bool f = ((nonid >> 2) & 1u) != 0u && e1 >= 2 && e0 <= n - 3;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int p = k < 2 ? k : n - 4 + k;
-        if (p >= e0 && p <= e1 && p >= 0) f |= ((nonid >> pos_class(p, n)) & 1u) != 0u;
-    }
-    return f;
-}
 
 // v <- M v along direction D of a 27-vector v[az*9 + ay*3 + ax], M = R (TR false) or R^T (TR true)
 template <int D, bool TR>
@@ -235,7 +210,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
     __shared__ float s_r[3][5][9];
-    __shared__ unsigned s_nonid[3];
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -244,7 +218,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         tc::tmem_relinquish();
     }
     for (int i = tid; i < 3 * 5 * 9; i += kPtThreads) (&s_r[0][0][0])[i] = (&xf.r[0][0][0])[i];
-    if (tid < 3) s_nonid[tid] = xf.nonid[tid];
     if (tid == 0) {
         tc::mbar_init(&a_full[0], kRoleThreads);
         tc::mbar_init(&a_full[1], kRoleThreads);
@@ -372,7 +345,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         // lanes, along y by 8 and 16 lanes; the 4 layers are combined through shared memory.
         const int et = tid - kRoleThreads;
         const int c = (warp - kRoleWarps) >> 2, q = warp & 3;
-        const int r = q * 32 + lane;
         const int lx = lane & 7, ly = lane >> 3;
         const uint32_t dcol0 = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kColD + c * 32);
         const unsigned FULL = 0xffffffffu;

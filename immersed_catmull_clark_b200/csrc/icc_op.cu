@@ -257,6 +257,7 @@ Op::~Op() {
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
     mixed_release(*this);
+    state_release(*this);
 }
 
 int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type_id, const double *scale,
@@ -379,6 +380,12 @@ int Op::set_scale(const double *scale) {
     host_scale.assign(src, src + nel);
     ICC_CUDA(cudaMemcpyAsync(d_scale, src, (size_t)nel * 8, cudaMemcpyHostToDevice, stream), "copy scale");
     ICC_CUDA(cudaStreamSynchronize(stream), "copy scale");
+    scale_version++;
+    return mixed_on_scale_update(*this);
+}
+
+int Op::set_scale_dev(const double *scale_dev) {
+    ICC_CUDA(cudaMemcpyAsync(d_scale, scale_dev, (size_t)nel * 8, cudaMemcpyDeviceToDevice, stream), "copy scale");
     scale_version++;
     return mixed_on_scale_update(*this);
 }
@@ -507,10 +514,6 @@ int Op::pcg_fp64(const double *b, const double *diag, double tol, int64_t max_it
 // ------------------------------------------------------------------------------------------
 using icc::set_error;
 
-struct icc_op {
-    icc::Op op;
-};
-
 extern "C" {
 
 const char *icc_last_error(void) { return icc::g_last_error.c_str(); }
@@ -614,7 +617,7 @@ int icc_op_diagonal(icc_op *op, double *d, int64_t n) {
     return ICC_OK;
 }
 
-static int solve_common(icc_op *op, const double *b_dev, const double *diag_dev, int64_t n, double tol,
+int icc_solve_common(icc_op *op, const double *b_dev, const double *diag_dev, int64_t n, double tol,
                         int64_t max_iter, const icc_solve_opts *opts, double *x_dev, int64_t *iters, double *rel_res) {
     icc::Op &o = op->op;
     if (n != o.ndof) return set_error(ICC_BAD_ARG, "icc_pcg_solve: n != ndof");
@@ -646,7 +649,7 @@ int icc_pcg_solve_dev(icc_op *op, const double *b_dev, const double *diag_dev, i
                       int64_t max_iter, const icc_solve_opts *opts, double *x_dev, int64_t *iters, double *rel_res) {
     if (!op || !b_dev || !x_dev) return set_error(ICC_BAD_ARG, "icc_pcg_solve_dev: null argument");
     cudaSetDevice(op->op.device);
-    int rc = solve_common(op, b_dev, diag_dev, n, tol, max_iter, opts, x_dev, iters, rel_res);
+    int rc = icc_solve_common(op, b_dev, diag_dev, n, tol, max_iter, opts, x_dev, iters, rel_res);
     cudaError_t e = cudaStreamSynchronize(op->op.stream);
     if (e != cudaSuccess && rc >= 0) return icc::set_error(ICC_CUDA_ERROR, cudaGetErrorString(e));
     return rc;
@@ -662,7 +665,7 @@ int icc_pcg_solve(icc_op *op, const double *b, const double *diag, int64_t n, do
     if (rc) return rc;
     ICC_CUDA(cudaMemcpyAsync(o.d_b, b, (size_t)n * 8, cudaMemcpyHostToDevice, o.stream), "solve h2d");
     if (diag) ICC_CUDA(cudaMemcpyAsync(o.d_diag, diag, (size_t)n * 8, cudaMemcpyHostToDevice, o.stream), "solve h2d");
-    rc = solve_common(op, o.d_b, diag ? o.d_diag : nullptr, n, tol, max_iter, opts, o.d_y_out, iters, rel_res);
+    rc = icc_solve_common(op, o.d_b, diag ? o.d_diag : nullptr, n, tol, max_iter, opts, o.d_y_out, iters, rel_res);
     if (rc < 0) return rc;
     ICC_CUDA(cudaMemcpyAsync(x, o.d_y_out, (size_t)n * 8, cudaMemcpyDeviceToHost, o.stream), "solve d2h");
     ICC_CUDA(cudaStreamSynchronize(o.stream), "solve sync");

@@ -150,6 +150,42 @@ int icc_apply_f64_noalloc(const int64_t nel_dir[3], const double *ke_types_dev, 
                           const int32_t *type_id_dev, const double *scale_dev, const double *x_dev, double *y_dev,
                           void *stream);
 
+/* ---- callers of the path in the SIMP loop ------------------------------------------------------
+ * rust/src/topopt_iga.rs:137-162 CantileverTopOpt::solve_state on the handle's operator (mask mode
+ * ICC_MASK_ZERO = the reference's closure): b = F - K u0 on free DOFs, diag clamped at 1e-12,
+ * tol' = min(pcg_tol |F_free| / |b|, 0.5) (1 when b = 0), du from the PCG (opts->precision selects
+ * FP64 or MIXED), u = u0 + du on free DOFs and 0 on fixed ones; *rel_res = PCG residual * |b| /
+ * |F_free| as the reference returns it.  u0 must vanish on fixed DOFs.  Host arrays of n = ndof;
+ * u may alias u0. */
+int icc_solve_state(icc_op *op, const double *force, const double *u0, int64_t n, double pcg_tol,
+                    const icc_solve_opts *opts, double *u, int64_t *iters, double *rel_res);
+
+/* rust/src/topopt_iga.rs:165-184 element_energies: ee[e] = u_e^T K_type(e) u_e (unscaled). */
+int icc_op_element_energies(icc_op *op, const double *u, int64_t n, double *ee, int64_t nel);
+
+/* rust/src/topopt_iga.rs:19-54 CantileverTopOptConfig (nel and degree 2 are arguments). */
+typedef struct icc_topopt_cfg {
+    double size[3];           /* box [0,size0] x [0,size1] x [0,size2] (reference default 1.2, 0.6, 0.3) */
+    double volfrac, penal, rmin, young, poisson, emin, move_limit, pcg_tol;
+    int32_t precision;        /* state solves: ICC_FP64 or ICC_MIXED */
+    int32_t reserved;
+} icc_topopt_cfg;
+
+typedef struct icc_topopt icc_topopt;
+
+/* rust/src/topopt_iga.rs:73-129 CantileverTopOpt::new: clamp x = 0, the reference's tip load, the
+ * radius filter on element centres (as a stencil), the device operator. */
+int icc_topopt_create(const int64_t nel[3], const icc_topopt_cfg *cfg, icc_topopt **out);
+void icc_topopt_destroy(icc_topopt *t);
+
+/* rust/src/topopt_iga.rs:187-234 CantileverTopOpt::run: densities from volfrac, per iteration the
+ * SIMP scale, the warm-started state solve, compliance |F'u|, sensitivities, filter and the OC
+ * bisection (candidate of its last step); stops after max_iter or when change < 0.01 and
+ * iteration >= 15.  Outputs per iteration (arrays of max_iter; any may be NULL): compliance,
+ * change, PCG iterations; final densities (nel); iterations run. */
+int icc_topopt_run(icc_topopt *t, int32_t max_iter, double *compliance, double *change, int64_t *pcg_iters,
+                   double *density, int32_t *iters_run);
+
 /* ---- diagnostics (no reference counterpart) -------------------------------------------------
  * Times `reps` FP64 applies of x_dev on the handle's stream with CUDA events around each of the
  * two kernels of an apply (the element-brick contraction and the node-side sum); returns the
