@@ -44,7 +44,7 @@ EXPORTED = [
     "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
     "icc_op_profile_apply_f32", "icc_solve_state", "icc_op_element_energies", "icc_topopt_create",
-    "icc_topopt_destroy", "icc_topopt_run",
+    "icc_topopt_destroy", "icc_topopt_run", "icc_cylinder_weights",
     "icc_apply_f64_noalloc",
 ]
 
@@ -124,6 +124,7 @@ def lib():
     L.icc_topopt_destroy.argtypes = [vp]
     L.icc_topopt_destroy.restype = None
     L.icc_topopt_run.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(i32)]
+    L.icc_cylinder_weights.argtypes = [i64p, i32p, dbl, f64p, vp]
     _lib = L
     return L
 
@@ -377,3 +378,15 @@ class CantileverTopOpt:
         _check(lib().icc_topopt_run(self._h, max_iter, _vp(comp), _vp(chg), _vp(its), _vp(dens), C.byref(done)))
         k = done.value
         return TopOptHistory(comp[:k], chg[:k], its[:k], dens)
+
+
+def cylinder_weights(res, sub, radius):
+    """Volume fraction and status (1 inside, 0 outside, -1 cut) of every cell of the unit cube minus
+    three orthogonal through-cylinders (rust/src/immersed.rs:88-155 rule), computed on the device."""
+    ncell = int(np.prod(res))
+    w = np.zeros(ncell)
+    st = np.zeros(ncell, dtype=np.int8)
+    _check(lib().icc_cylinder_weights(np.ascontiguousarray(res, dtype=np.int64),
+                                      np.ascontiguousarray(sub, dtype=np.int32), float(radius), w,
+                                      st.ctypes.data_as(C.c_void_p)))
+    return w, st

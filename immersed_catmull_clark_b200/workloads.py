@@ -1,4 +1,5 @@
-"""Synthetic inputs of the benchmark configurations (numpy only; seeded PCG64).
+"""Synthetic inputs of the benchmark configurations (numpy, seeded PCG64; the immersed volume
+fractions come from the library's device kernel).
 
 * cantilever(nel, smooth):  the SIMP cantilever on the box [0,2] x [0,1] x [0,1]: E0 = 1,
   E_min = 1e-9, nu = 0.3, SIMP penalty 3, densities i.i.d. U[0.01, 1] (optionally smoothed by a
@@ -11,8 +12,8 @@
   1e-3 inactive, alpha floored at 1e-6, clamped at z = 0, pressure 1 on the z = 1 face.
 
 The element scale follows the reference: s_e = E_min + rho^p (E0 - E_min) (rust/src/topopt_iga.rs:132
-with E0 folded into the Lame parameters), times alpha for immersed cells
-(rust/src/topopt_immersed.rs:166).
+with E0 folded into the Lame parameters); immersed cells use E_min + rho^p (E0 - E_min) alpha_e
+(rust/src/immersed.rs:484, rust/src/topopt_immersed.rs:166) and inactive cells none.
 """
 from dataclasses import dataclass
 
@@ -95,21 +96,10 @@ def _cyl_inside(x, y, z, r):
 
 
 def cylinder_fractions(n, sub=8, radius=0.25):
-    """Per-cell volume fraction and status (1 inside, 0 outside, -1 cut) on an n^3 grid of [0,1]^3."""
-    xs = np.linspace(0.0, 1.0, n + 1)
-    xs[-1] = 1.0
-    Z, Y, X = np.meshgrid(xs, xs, xs, indexing="ij")
-    ins = _cyl_inside(X, Y, Z, radius).astype(np.int32)
-    cnt = sum(ins[dz:dz + n, dy:dy + n, dx:dx + n] for dz in (0, 1) for dy in (0, 1) for dx in (0, 1))
-    status = np.where(cnt == 8, 1, np.where(cnt == 0, 0, -1)).astype(np.int8)
-    w = np.where(status == 1, 1.0, 0.0)
-    h = 1.0 / n
-    cut = np.argwhere(status == -1)
-    off = (np.arange(sub) + 0.5) * (h / sub)
-    for k, j, i in cut:
-        zz, yy, xx = np.meshgrid(k * h + off, j * h + off, i * h + off, indexing="ij")
-        w[k, j, i] = _cyl_inside(xx, yy, zz, radius).sum() / float(sub ** 3)
-    return w.reshape(-1), status.reshape(-1)
+    """Per-cell volume fraction and status (1 inside, 0 outside, -1 cut) on an n^3 grid of [0,1]^3
+    (rust/src/immersed.rs:88-155 rule), computed by the library's device kernel."""
+    from . import cylinder_weights
+    return cylinder_weights((n, n, n), (sub, sub, sub), radius)
 
 
 def cylinders(n=96, sub=8, radius=0.25, name=None):
@@ -118,7 +108,8 @@ def cylinders(n=96, sub=8, radius=0.25, name=None):
     alpha = alpha.astype(np.float32).astype(np.float64)   # stored in FP32
     active = alpha >= 1e-3
     a = np.where(active, np.maximum(alpha, 1e-6), 0.0)
-    scale = (EMIN + 1.0 * (E0 - EMIN)) * a               # density 1
+    # s_e = E_min + rho^p (E0 - E_min) alpha_e on active cells (density 1), no stiffness elsewhere
+    scale = np.where(active, EMIN + (E0 - EMIN) * a, 0.0)
     cx = cy = cz = n + 2
     nsc = cx * cy * cz
     # control points touched by no active cell carry no stiffness: mask them out

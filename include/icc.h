@@ -186,6 +186,15 @@ void icc_topopt_destroy(icc_topopt *t);
 int icc_topopt_run(icc_topopt *t, int32_t max_iter, double *compliance, double *change, int64_t *pcg_iters,
                    double *density, int32_t *iters_run);
 
+/* ---- immersed set-up ------------------------------------------------------------------------------
+ * rust/src/immersed.rs:88-155 classify_background_cells + element_weights on the res[0] x res[1] x
+ * res[2] grid of the unit cube for the analytic solid "cube minus three orthogonal through-cylinders
+ * of radius `radius` about the centre lines" (the reference evaluates a triangle mesh by ray parity;
+ * the rule is the same): status 1 inside, 0 outside, -1 cut; weight 1, 0, or the fraction of
+ * sub[0] x sub[1] x sub[2] cell midpoints inside.  Computed on the device; host arrays of
+ * res[0] res[1] res[2] cells. */
+int icc_cylinder_weights(const int64_t res[3], const int32_t sub[3], double radius, double *weights, int8_t *status);
+
 /* ---- diagnostics (no reference counterpart) -------------------------------------------------
  * Times `reps` FP64 applies of x_dev on the handle's stream with CUDA events around each of the
  * two kernels of an apply (the element-brick contraction and the node-side sum); returns the
