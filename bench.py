@@ -41,7 +41,15 @@ WORKLOADS = {
     "cantilever128": dict(nel=(128, 64, 64), smooth=True),
     "cantilever24": dict(nel=(24, 16, 12), smooth=False),
     "cantilever256": dict(nel=(256, 128, 128), smooth=True),
+    # the immersed case: unit cube minus three r = 0.25 cylinders, 96^3 cells, Jacobi clamp 1e-6
+    "cylinders96": dict(kind="cylinders", n=96),
 }
+
+
+def make_problem(W, wl, seed):
+    if wl.get("kind") == "cylinders":
+        return W.cylinders(wl["n"])
+    return W.cantilever(wl["nel"], smooth=wl["smooth"], seed=seed)
 
 
 def parse():
@@ -182,7 +190,7 @@ def run_reference(args):
     from oracle import oracle as O
     O.build()
     wl = WORKLOADS[args.workload]
-    prob = W.cantilever(wl["nel"], smooth=wl["smooth"], seed=SEED)
+    prob = make_problem(W, wl, SEED)
     per_step = max(2.0, min(10.0, args.cpu_seconds))
     vals = []
     for i in range(args.warmup + args.steps):
@@ -215,7 +223,7 @@ def run_ours(args):
     from immersed_catmull_clark_b200 import workloads as W
 
     wl = WORKLOADS[args.workload]
-    prob = W.cantilever(wl["nel"], smooth=wl["smooth"], seed=SEED + rank)
+    prob = make_problem(W, wl, SEED + rank)
     sp = icc.SpaceBox(prob.bounds, prob.nel, 2)
     lam, mu = icc.lame(W.E0, W.NU)
     em = icc.elasticity_element_matrices(sp, lam, mu)
@@ -224,6 +232,13 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(op.stream, device=dev)
     b_host = W.rhs_masked(prob)
     b_dev = torch.from_numpy(b_host).to(dev)
+    # Jacobi diagonal: the operator's own (0) for the cantilever; clamped at 1e-6 for the immersed
+    # case as the reference does (rust/src/immersed.rs:555)
+    diag_host, diag_ptr = None, 0
+    if wl.get("kind") == "cylinders":
+        diag_host = np.maximum(op.diagonal(), 1e-6)
+        diag_t = torch.from_numpy(diag_host).to(dev)
+        diag_ptr = diag_t.data_ptr()
     x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     precision = icc.MIXED if args.mode == "mixed" else icc.FP64
@@ -259,7 +274,7 @@ def run_ours(args):
 
     def timed_solves(slv, steps, warmup, x_out):
         for _ in range(warmup):
-            slv.solve_dev(n, b_dev.data_ptr(), 0, x_out.data_ptr(), op)
+            slv.solve_dev(n, b_dev.data_ptr(), diag_ptr, x_out.data_ptr(), op)
         barrier()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         iters, launches = [], 0
@@ -267,7 +282,7 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 ev[i][0].record(stream)
-            it, res = slv.solve_dev(n, b_dev.data_ptr(), 0, x_out.data_ptr(), op)
+            it, res = slv.solve_dev(n, b_dev.data_ptr(), diag_ptr, x_out.data_ptr(), op)
             with torch.cuda.stream(stream):
                 ev[i][1].record(stream)
             iters.append(int(it))
@@ -339,7 +354,7 @@ def run_ours(args):
             flush.zero_()
             e0.record(stream)
         op.update_scale(s_pin.numpy())
-        it, res = solver.solve_host_ptr(n, b_pin.numpy(), None, x_pin.numpy(), op)
+        it, res = solver.solve_host_ptr(n, b_pin.numpy(), diag_host, x_pin.numpy(), op)
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()
@@ -352,7 +367,7 @@ def run_ours(args):
     if not args.no_ref_solution:
         x_ref = torch.zeros_like(x_dev)
         ref_solver = icc.PcgSolver(40 * n, 1e-12, precision=icc.FP64)
-        it_ref, res_ref = ref_solver.solve_dev(n, b_dev.data_ptr(), 0, x_ref.data_ptr(), op)
+        it_ref, res_ref = ref_solver.solve_dev(n, b_dev.data_ptr(), diag_ptr, x_ref.data_ptr(), op)
         xr, xs = x_ref.cpu().numpy(), x_dev.cpu().numpy()
         c_ref, c = float(prob.force @ xr), float(prob.force @ xs)
         err = {"disp_rel_l2": float(np.linalg.norm(xs - xr) / np.linalg.norm(xr)),
@@ -376,7 +391,7 @@ def run_ours(args):
         cpu.pop("seconds", None)
 
     if rank == 0:
-        cfg = {"workload": f"{prob.name} SIMP cantilever, smoothed densities" if wl["smooth"] else prob.name,
+        cfg = {"workload": f"{prob.name} SIMP cantilever, smoothed densities" if wl.get("smooth") else prob.name,
                "ndof": n, "nel": sp.nel, "tol": TOL, "seed": SEED, "mode": args.mode,
                "iterations": iters, "time_to_tol_ms": ms_steps,
                "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
@@ -391,7 +406,8 @@ def run_ours(args):
                             "algorithmic_flops_per_launch": flops, "launch_ms": contract_ms,
                             "node_sum_kernel_ms": gather_ms, "peak_source": peak_src},
                "cpu_baseline": cpu,
-               "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n + 8 * sp.nel,
+               "e2e": {"value": e2e_value, "unit": UNIT,
+                       "h2d_bytes_per_step": 8 * n + 8 * sp.nel + (8 * n if diag_host is not None else 0),
                        "d2h_bytes_per_step": 8 * n},
                "gpu_launches": int(launches),
                "clocks": clk.summary(),
