@@ -44,7 +44,7 @@ EXPORTED = [
     "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
     "icc_op_profile_apply_f32", "icc_solve_state", "icc_op_element_energies", "icc_topopt_create",
-    "icc_topopt_destroy", "icc_topopt_run", "icc_cylinder_weights",
+    "icc_topopt_destroy", "icc_topopt_run", "icc_cylinder_weights", "icc_pcg_solve_batched",
     "icc_apply_f64_noalloc",
 ]
 
@@ -125,6 +125,7 @@ def lib():
     L.icc_topopt_destroy.restype = None
     L.icc_topopt_run.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(i32)]
     L.icc_cylinder_weights.argtypes = [i64p, i32p, dbl, f64p, vp]
+    L.icc_pcg_solve_batched.argtypes = [i32, vp, vp, vp, dbl, i64, C.POINTER(SolveOpts), vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -390,3 +391,24 @@ def cylinder_weights(res, sub, radius):
                                       np.ascontiguousarray(sub, dtype=np.int32), float(radius), w,
                                       st.ctypes.data_as(C.c_void_p)))
     return w, st
+
+
+def solve_batched(ops, bs, diags=None, tol=1e-8, max_iter=None, precision=FP64, check_every=32):
+    """Independent solves ops[i] x_i = bs[i], all in flight together (icc_pcg_solve_batched).
+    Returns (xs, iterations, rel_res, status) per instance."""
+    k = len(ops)
+    xs = [np.zeros(op.n) for op in ops]
+    bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+    ds = None if diags is None else [np.ascontiguousarray(d, dtype=np.float64) for d in diags]
+    hv = (C.c_void_p * k)(*[op._h.value for op in ops])
+    bv = (C.c_void_p * k)(*[b.ctypes.data for b in bs])
+    xv = (C.c_void_p * k)(*[x.ctypes.data for x in xs])
+    dv = None if ds is None else (C.c_void_p * k)(*[d.ctypes.data for d in ds])
+    its = np.zeros(k, dtype=np.int64)
+    res = np.zeros(k)
+    st = np.zeros(k, dtype=np.int32)
+    mi = max_iter if max_iter is not None else 20 * max(op.n for op in ops)
+    opts = SolveOpts(precision, check_every, 0.0, 0, 0)
+    _check(lib().icc_pcg_solve_batched(k, hv, bv, dv, tol, mi, C.byref(opts), xv, its.ctypes.data,
+                                       res.ctypes.data, st.ctypes.data))
+    return xs, its, res, st

@@ -884,7 +884,10 @@ static int mixed_init(Op &op) {
         int per_sm = 0;
         ICC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_tail_kernel, kTailThreads, 0),
                  "tail occupancy");
-        ms.tail_grid = std::max(1, std::min(per_sm, 4)) * op.num_sms;
+        // every CTA must be resident (grid barriers); small grids take only the CTAs they need, so
+        // the fused steps of concurrent solves (icc_pcg_solve_batched) can share the GPU
+        const long long need = (op.g.nsc + kTailThreads - 1) / kTailThreads;
+        ms.tail_grid = (int)std::max(1LL, std::min<long long>((long long)std::max(1, std::min(per_sm, 4)) * op.num_sms, need));
         if ((rc = dalloc(&ms.d_tail_part, (size_t)3 * ms.tail_grid, "alloc mixed"))) return rc;
         if ((rc = dalloc(&ms.d_grid_ctr, 1, "alloc mixed"))) return rc;
         ICC_CUDA(cudaMemset(ms.d_grid_ctr, 0, sizeof(unsigned long long)), "clear grid counter");

@@ -18,11 +18,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "icc_internal.h"
@@ -670,6 +672,44 @@ int icc_pcg_solve(icc_op *op, const double *b, const double *diag, int64_t n, do
     ICC_CUDA(cudaMemcpyAsync(x, o.d_y_out, (size_t)n * 8, cudaMemcpyDeviceToHost, o.stream), "solve d2h");
     ICC_CUDA(cudaStreamSynchronize(o.stream), "solve sync");
     return rc;
+}
+
+int icc_pcg_solve_batched(int32_t count, icc_op *const *ops, const double *const *b, const double *const *diag,
+                          double tol, int64_t max_iter, const icc_solve_opts *opts, double *const *x, int64_t *iters,
+                          double *rel_res, int32_t *status) {
+    if (count < 0 || (count > 0 && (!ops || !b || !x || !status)))
+        return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: null argument");
+    for (int32_t i = 0; i < count; ++i)
+        if (!ops[i] || !b[i] || !x[i]) return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: null instance argument");
+    // instances on worker threads, each solving on its handle's own stream: the GPU interleaves the
+    // instances' kernels (small grids leave SMs to the others); every solve is deterministic, so the
+    // results equal those of sequential calls
+    std::atomic<int32_t> next(0);
+    std::vector<std::string> errs((size_t)count);
+    auto work = [&]() {
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= count) return;
+            icc::Op &o = ops[i]->op;
+            cudaSetDevice(o.device);
+            int64_t it = 0;
+            double rr = 1.0;
+            const int rc = icc_pcg_solve(ops[i], b[i], diag ? diag[i] : nullptr, o.ndof, tol, max_iter, opts, x[i], &it,
+                                         &rr);
+            status[i] = rc;
+            if (iters) iters[i] = it;
+            if (rel_res) rel_res[i] = rr;
+            if (rc < 0) errs[(size_t)i] = icc_last_error();
+        }
+    };
+    const int32_t nthreads = std::max<int32_t>(1, std::min<int32_t>(count, 16));
+    std::vector<std::thread> pool;
+    for (int32_t t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    for (int32_t i = 0; i < count; ++i)
+        if (status[i] < 0) return set_error(status[i], "instance " + std::to_string(i) + ": " + errs[(size_t)i]);
+    return ICC_OK;
 }
 
 int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t reps, double *contract_ms,

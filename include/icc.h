@@ -150,6 +150,15 @@ int icc_apply_f64_noalloc(const int64_t nel_dir[3], const double *ke_types_dev, 
                           const int32_t *type_id_dev, const double *scale_dev, const double *x_dev, double *y_dev,
                           void *stream);
 
+/* Many independent solves (designs of uneven sizes, or load cases) at once: instance i solves
+ * ops[i] x[i] = b[i] as icc_pcg_solve does (diag may be NULL, or diag[i] NULL), all instances in
+ * flight together on their handles' streams.  Per instance: status[i] (an icc_pcg_solve code),
+ * iters[i], rel_res[i] (both may be NULL).  Returns ICC_OK when every instance ran (converged or
+ * not), else the first instance's error.  The handles must be distinct. */
+int icc_pcg_solve_batched(int32_t count, icc_op *const *ops, const double *const *b, const double *const *diag,
+                          double tol, int64_t max_iter, const icc_solve_opts *opts, double *const *x, int64_t *iters,
+                          double *rel_res, int32_t *status);
+
 /* ---- callers of the path in the SIMP loop ------------------------------------------------------
  * rust/src/topopt_iga.rs:137-162 CantileverTopOpt::solve_state on the handle's operator (mask mode
  * ICC_MASK_ZERO = the reference's closure): b = F - K u0 on free DOFs, diag clamped at 1e-12,
