@@ -45,6 +45,7 @@ EXPORTED = [
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
     "icc_op_profile_apply_f32", "icc_solve_state", "icc_op_element_energies", "icc_topopt_create",
     "icc_topopt_destroy", "icc_topopt_run", "icc_cylinder_weights", "icc_pcg_solve_batched",
+    "icc_topopt_set_loads",
     "icc_apply_f64_noalloc",
 ]
 
@@ -124,6 +125,7 @@ def lib():
     L.icc_topopt_destroy.argtypes = [vp]
     L.icc_topopt_destroy.restype = None
     L.icc_topopt_run.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(i32)]
+    L.icc_topopt_set_loads.argtypes = [vp, i32, f64p]
     L.icc_cylinder_weights.argtypes = [i64p, i32p, dbl, f64p, vp]
     L.icc_pcg_solve_batched.argtypes = [i32, vp, vp, vp, dbl, i64, C.POINTER(SolveOpts), vp, vp, vp, vp]
     _lib = L
@@ -371,6 +373,11 @@ class CantileverTopOpt:
         if h is not None and _lib is not None:
             _lib.icc_topopt_destroy(h)
             self._h = None
+
+    def set_loads(self, forces):
+        """Load cases as simultaneous right-hand sides (rows of forces, each of ndof)."""
+        f = np.ascontiguousarray(np.atleast_2d(forces), dtype=np.float64)
+        _check(lib().icc_topopt_set_loads(self._h, f.shape[0], f.reshape(-1)))
 
     def run(self, max_iter=40):
         comp, chg = np.zeros(max_iter), np.zeros(max_iter)

@@ -36,7 +36,7 @@ constexpr int kEnergyWarps = 8;
 // adds u_a * row_a; the warp sum is the energy.
 __global__ void __launch_bounds__(kEnergyWarps * 32)
 energies_kernel(Geom g, const double *__restrict__ K, const int *__restrict__ type_id, const double *__restrict__ u,
-                double *__restrict__ ee) {
+                double *__restrict__ ee, int accumulate) {
     __shared__ double su[kEnergyWarps][81];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long nel = (long long)g.nx * g.ny * g.nz;
@@ -56,7 +56,7 @@ energies_kernel(Geom g, const double *__restrict__ K, const int *__restrict__ ty
             s += su[warp][a] * row;
         }
         s = warp_sum(s);
-        if (lane == 0) ee[e] = s;
+        if (lane == 0) ee[e] = accumulate ? ee[e] + s : s;
         __syncwarp();
     }
 }
@@ -299,10 +299,12 @@ static int solve_state_dev(icc_op *h, StateScratch &s, const double *force, cons
     return rc;
 }
 
-static int energies_dev(Op &o, StateScratch &s, const double *u, double *ee) {
+// ee = u_e^T K_e u_e, or ee += it (several load cases)
+static int energies_dev(Op &o, StateScratch &s, const double *u, double *ee, bool accumulate = false) {
     int rc;
     if ((rc = state_ktypes(o, s))) return rc;
-    energies_kernel<<<o.num_sms * 8, kEnergyWarps * 32, 0, o.stream>>>(o.g, s.ktypes, o.d_type_id, u, ee);
+    energies_kernel<<<o.num_sms * 8, kEnergyWarps * 32, 0, o.stream>>>(o.g, s.ktypes, o.d_type_id, u, ee,
+                                                                      accumulate ? 1 : 0);
     ICC_CUDA(cudaGetLastError(), "energies");
     return ICC_OK;
 }
@@ -323,6 +325,7 @@ struct icc_topopt {
            *d_part = nullptr, *d_w = nullptr;
     int4 *d_off = nullptr;
     int nst = 0, nblocks = 0;
+    int nload = 1;   // load cases: d_force and d_u hold nload vectors of n
     ~icc_topopt() {
         void *p[] = {d_force, d_u, d_un, d_x, d_xold, d_cand, d_scale, d_ee, d_dcraw, d_dc, d_part, d_w, d_off};
         for (void *q : p)
@@ -450,6 +453,32 @@ int icc_topopt_create(const int64_t nel[3], const icc_topopt_cfg *cfg, icc_topop
 
 void icc_topopt_destroy(icc_topopt *t) { delete t; }
 
+int icc_topopt_set_loads(icc_topopt *t, int32_t nload, const double *forces) {
+    if (!t || nload < 1 || !forces) return icc::set_error(ICC_BAD_ARG, "icc_topopt_set_loads: bad argument");
+    icc::Op &o = t->op->op;
+    cudaSetDevice(o.device);
+    double *f = nullptr, *u = nullptr;
+    const size_t cnt = (size_t)nload * (size_t)t->n;
+    int rc;
+    if ((rc = icc::dalloc(&f, cnt, "alloc loads"))) return rc;
+    if ((rc = icc::dalloc(&u, cnt, "alloc loads"))) {
+        cudaFree(f);
+        return rc;
+    }
+    cudaError_t e = cudaMemcpy(f, forces, cnt * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(f);
+        cudaFree(u);
+        return icc::cuda_fail(e, "copy loads");
+    }
+    cudaFree(t->d_force);
+    cudaFree(t->d_u);
+    t->d_force = f;
+    t->d_u = u;
+    t->nload = nload;
+    return ICC_OK;
+}
+
 int icc_topopt_run(icc_topopt *t, int32_t max_iter, double *compliance, double *change, int64_t *pcg_iters,
                    double *density, int32_t *iters_run) {
     if (!t || max_iter < 0) return icc::set_error(ICC_BAD_ARG, "icc_topopt_run: bad argument");
@@ -464,21 +493,29 @@ int icc_topopt_run(icc_topopt *t, int32_t max_iter, double *compliance, double *
     if ((rc = icc::state_scratch(o, s))) return rc;
     const icc_solve_opts opts = {c.precision, 32, 0.0, 0, 0};
     icc::fill_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(ne, t->d_x, c.volfrac);
-    ICC_CUDA(cudaMemsetAsync(t->d_u, 0, (size_t)n * 8, o.stream), "zero u");
+    ICC_CUDA(cudaMemsetAsync(t->d_u, 0, (size_t)t->nload * n * 8, o.stream), "zero u");
     int done = 0;
     for (int iter = 1; iter <= max_iter; ++iter) {
         ICC_CUDA(cudaMemcpyAsync(t->d_xold, t->d_x, (size_t)ne * 8, cudaMemcpyDeviceToDevice, o.stream), "x_old");
         icc::simp_scale_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(ne, t->d_x, c.emin, c.penal, t->d_scale);
         if ((rc = o.set_scale_dev(t->d_scale))) return rc;
+        // every load case: warm-started state, compliance F'u and energies, summed over the cases
         int64_t it = 0;
-        double res = 0.0;
-        rc = icc::solve_state_dev(t->op, s, t->d_force, t->d_u, c.pcg_tol, &opts, t->d_un, &it, &res);
-        if (rc < 0) return rc;
-        std::swap(t->d_u, t->d_un);
         double comp = 0.0;
-        icc::dot_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(n, t->d_force, t->d_u, t->d_part);
-        if ((rc = icc::reduce_to_host(o, s, t->d_part, nb, 0, &comp))) return rc;
-        if ((rc = icc::energies_dev(o, s, t->d_u, t->d_ee))) return rc;
+        for (int k = 0; k < t->nload; ++k) {
+            double *fk = t->d_force + (size_t)k * n, *uk = t->d_u + (size_t)k * n;
+            int64_t itk = 0;
+            double res = 0.0;
+            rc = icc::solve_state_dev(t->op, s, fk, uk, c.pcg_tol, &opts, t->d_un, &itk, &res);
+            if (rc < 0) return rc;
+            it += itk;
+            ICC_CUDA(cudaMemcpyAsync(uk, t->d_un, (size_t)n * 8, cudaMemcpyDeviceToDevice, o.stream), "state copy");
+            double ck = 0.0;
+            icc::dot_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(n, fk, uk, t->d_part);
+            if ((rc = icc::reduce_to_host(o, s, t->d_part, nb, 0, &ck))) return rc;
+            comp += ck;
+            if ((rc = icc::energies_dev(o, s, uk, t->d_ee, k > 0))) return rc;
+        }
         icc::sens_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(ne, t->d_x, t->d_ee, c.emin, c.penal, t->d_dcraw);
         icc::filter_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(o.g, t->nst, t->d_off, t->d_w, t->d_x, t->d_dcraw,
                                                                    t->d_dc, t->d_part);

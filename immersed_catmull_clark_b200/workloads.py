@@ -187,3 +187,53 @@ def _bspline2(kn, i, x):
 
 def rhs_masked(p: Problem):
     return np.where(p.free_mask > 0, p.force, 0.0)
+
+
+def _first_moments(nel, length, x0):
+    """int_0^L N_i(x) (x - x0) dx for the p = 2 open uniform basis (3-point Gauss per element)."""
+    kn = np.concatenate([[0.0, 0.0, 0.0], np.arange(1, nel) / nel, [1.0, 1.0, 1.0]])
+    gx, gw = np.polynomial.legendre.leggauss(3)
+    m = np.zeros(nel + 2)
+    h = 1.0 / nel
+    for e in range(nel):
+        for t, w in zip(gx, gw):
+            u = (e + 0.5 * (t + 1.0)) * h            # parameter in [0, 1]
+            for r in range(3):
+                m[e + r] += w * 0.5 * h * length * _bspline2(kn, e + r, u) * (u * length - x0)
+    return m
+
+
+def tip_load_cases(nel, size=(2.0, 1.0, 1.0)):
+    """Four consistent load cases on the tip face x = size0 of the clamped cantilever box: shear +y,
+    shear -y and axial +x (unit total force each, uniform traction) and a torsion couple about the
+    face's centre line (traction tau (0, -(z - zc), y - yc) with unit moment).  [4, ndof]."""
+    nx, ny, nz = nel
+    cx, cy, cz = nx + 2, ny + 2, nz + 2
+    nsc = cx * cy * cz
+    iy, iz = open_knot_integrals(ny, size[1]), open_knot_integrals(nz, size[2])
+    my, mz = _first_moments(ny, size[1], 0.5 * size[1]), _first_moments(nz, size[2], 0.5 * size[2])
+    area = size[1] * size[2]
+    polar = area * (size[1] ** 2 + size[2] ** 2) / 12.0     # int (y - yc)^2 + (z - zc)^2 dA
+    tau = 1.0 / polar
+    loads = np.zeros((4, 3 * nsc))
+    for k, (comp, val) in enumerate([(1, 1.0), (1, -1.0), (0, 1.0)]):
+        f = loads[k, comp * nsc:(comp + 1) * nsc].reshape(cz, cy, cx)
+        f[:, :, cx - 1] = val / area * np.outer(iz, iy)
+    fy = loads[3, nsc:2 * nsc].reshape(cz, cy, cx)
+    fz = loads[3, 2 * nsc:].reshape(cz, cy, cx)
+    fy[:, :, cx - 1] = -tau * np.outer(mz, iy)
+    fz[:, :, cx - 1] = tau * np.outer(iz, my)
+    return loads
+
+
+def reference_tip_load(nel):
+    """The reference cantilever's load (rust/src/topopt_iga.rs:78-97): -1/count in y on the control
+    points with i1 = last, |i2 - 1| <= 1, |i3 - ncp3/2| <= 1 (1-based)."""
+    nd = [n + 2 for n in nel]
+    nsc = nd[0] * nd[1] * nd[2]
+    idx = np.arange(nsc)
+    s0, s1, s2 = idx % nd[0], (idx // nd[0]) % nd[1], idx // (nd[0] * nd[1])
+    sel = (s0 + 1 == nd[0]) & (np.abs(s1 + 1.0 - 1.0) <= 1.0) & (np.abs(s2 + 1.0 - nd[2] / 2.0) <= 1.0)
+    f = np.zeros(3 * nsc)
+    f[nsc + idx[sel]] = -1.0 / sel.sum()
+    return f

@@ -89,3 +89,32 @@ def test_element_energies_match_oracle():
     assert np.abs(ee - ref).max() < 1e-12 * np.abs(ref).max()
     # energy identity: sum_e s_e ee_e = u' K u with the scaled operator
     assert abs(p.scale @ ee - u @ op.matvec(u)) < 1e-12 * abs(u @ op.matvec(u))
+
+
+def test_topopt_duplicate_load_case():
+    # the same load twice: compliance doubles, the OC update is unchanged (sensitivities scale by
+    # exactly 2), so the densities are bitwise those of the single case
+    nel = [12, 6, 4]
+    single = icc.CantileverTopOpt(nel, pcg_tol=1e-10)
+    h1 = single.run(4)
+    f = W.reference_tip_load(nel)
+    double = icc.CantileverTopOpt(nel, pcg_tol=1e-10)
+    double.set_loads(np.stack([f, f]))
+    h2 = double.run(4)
+    assert np.allclose(h2.compliance, 2 * h1.compliance, rtol=1e-12, atol=0)
+    assert np.array_equal(h2.density, h1.density)
+
+
+def test_topopt_four_load_cases_mixed_vs_fp64():
+    # four tip load cases (shear +-y, axial +x, torsion) as simultaneous right-hand sides
+    nel = [16, 8, 8]
+    loads = W.tip_load_cases(nel, size=(2.0, 1.0, 1.0))
+    runs = []
+    for prec in (icc.FP64, icc.MIXED):
+        t = icc.CantileverTopOpt(nel, size=(2.0, 1.0, 1.0), pcg_tol=1e-8, precision=prec)
+        t.set_loads(loads)
+        runs.append(t.run(4))
+    h64, hmx = runs
+    assert np.all(np.abs(hmx.compliance - h64.compliance) / h64.compliance < 1e-6)
+    assert np.abs(hmx.density - h64.density).max() < 1e-4
+    assert np.all(h64.compliance[1:] < h64.compliance[0])
