@@ -856,7 +856,7 @@ static int mixed_init(Op &op) {
     }
     int rc;
     if ((rc = dalloc(&ms.d_bmat, bm.size() / 4, "alloc tc matrices"))) return rc;
-    ICC_CUDA(cudaMemcpy(ms.d_bmat, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice), "copy tc matrices");
+    ICC_CUDA(cudaMemcpyAsync(ms.d_bmat, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice, op.stream), "copy tc matrices");
     const Geom &g = op.g;
     {
         std::vector<uint8_t> fl((size_t)g.nbricks, 0);
@@ -868,7 +868,8 @@ static int mixed_init(Op &op) {
                     if ((ms.xf.nonid[d] >> pos_class(e, n[d])) & 1u) fl[(size_t)b] |= uint8_t(1u << d);
         }
         if ((rc = dalloc(&ms.d_bflags, fl.size(), "alloc brick flags"))) return rc;
-        ICC_CUDA(cudaMemcpy(ms.d_bflags, fl.data(), fl.size(), cudaMemcpyHostToDevice), "copy brick flags");
+        ICC_CUDA(cudaMemcpyAsync(ms.d_bflags, fl.data(), fl.size(), cudaMemcpyHostToDevice, op.stream), "copy brick flags");
+        ICC_CUDA(cudaStreamSynchronize(op.stream), "copy brick flags");
     }
     const size_t n = (size_t)op.ndof;
     if ((rc = dalloc(&ms.d_scale32, (size_t)op.nel, "alloc mixed"))) return rc;
@@ -890,13 +891,14 @@ static int mixed_init(Op &op) {
         ms.tail_grid = (int)std::max(1LL, std::min<long long>((long long)std::max(1, std::min(per_sm, 4)) * op.num_sms, need));
         if ((rc = dalloc(&ms.d_tail_part, (size_t)3 * ms.tail_grid, "alloc mixed"))) return rc;
         if ((rc = dalloc(&ms.d_grid_ctr, 1, "alloc mixed"))) return rc;
-        ICC_CUDA(cudaMemset(ms.d_grid_ctr, 0, sizeof(unsigned long long)), "clear grid counter");
+        ICC_CUDA(cudaMemsetAsync(ms.d_grid_ctr, 0, sizeof(unsigned long long), op.stream), "clear grid counter");
     }
     if ((rc = dalloc(&ms.d_err, 1, "alloc mixed"))) return rc;
     if ((rc = dalloc(&ms.d_state, 1, "alloc mixed"))) return rc;
     ICC_CUDA(cudaMallocHost((void **)&ms.h_state, sizeof(PcgState)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&ms.h_scalars, 8 * sizeof(double)), "alloc pinned");
-    ICC_CUDA(cudaMemset(ms.d_err, 0, sizeof(int)), "clear err");
+    ICC_CUDA(cudaMemsetAsync(ms.d_err, 0, sizeof(int), op.stream), "clear err");
+    ICC_CUDA(cudaStreamSynchronize(op.stream), "clear err");
     ICC_CUDA(cudaFuncSetAttribute(apply_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPtSmem),
              "cudaFuncSetAttribute tc");
     ms.ready = true;
@@ -1017,7 +1019,8 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     for (auto &x2 : ev) cudaEventDestroy(x2);
     ICC_CUDA(e, "profile tc apply");
     int err = 0;
-    ICC_CUDA(cudaMemcpy(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
+    ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
     if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
     *contract_ms = a / reps;
     *gather_ms = gt / reps;
@@ -1143,6 +1146,9 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     int64_t updates = 0, launched = 0;
     double res = 1.0, best = INFINITY;
     int no_progress = 0;
+    // give up after the FP32 recurrence has gained eight decades (8 ln 0.1 / ln delta replacements)
+    // without a 10% improvement of the true residual
+    const int max_no_progress = std::max(8, (int)std::ceil(8.0 * std::log(0.1) / std::log(std::fmin(delta, 0.99))));
     for (;;) {
         ICC_CUDA(cudaGraphLaunch(ms.graph, op.stream), "graph launch");
         launches += 2 * int64_t(check_every);
@@ -1187,7 +1193,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         if (res < 0.9 * best) {
             best = res;
             no_progress = 0;
-        } else if (++no_progress >= 8) {
+        } else if (++no_progress >= max_no_progress) {
             break;  // FP32 recurrence no longer reduces the true residual: NOT_CONVERGED
         }
         ru_replace_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r64, 1.0 / sigma, ms.d_inv32, ms.d_r32,
@@ -1202,7 +1208,8 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         launches += 4;
     }
     int err = 0;
-    ICC_CUDA(cudaMemcpy(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
+    ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
     if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
     ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
     *iters = ms.h_state->iter;

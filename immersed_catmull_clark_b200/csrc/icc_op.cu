@@ -306,10 +306,10 @@ int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type
     int rc;
     if ((rc = dev_alloc(&d_kfrag, kf.size(), "alloc kfrag"))) return rc;
     if ((rc = dev_alloc(&d_kdiag, kd.size(), "alloc kdiag"))) return rc;
-    ICC_CUDA(cudaMemcpy(d_kfrag, kf.data(), kf.size() * 8, cudaMemcpyHostToDevice), "copy kfrag");
-    ICC_CUDA(cudaMemcpy(d_kdiag, kd.data(), kd.size() * 8, cudaMemcpyHostToDevice), "copy kdiag");
+    ICC_CUDA(cudaMemcpyAsync(d_kfrag, kf.data(), kf.size() * 8, cudaMemcpyHostToDevice, stream), "copy kfrag");
+    ICC_CUDA(cudaMemcpyAsync(d_kdiag, kd.data(), kd.size() * 8, cudaMemcpyHostToDevice, stream), "copy kdiag");
     if ((rc = dev_alloc(&d_type_id, (size_t)nel, "alloc type_id"))) return rc;
-    ICC_CUDA(cudaMemcpy(d_type_id, type_id, (size_t)nel * 4, cudaMemcpyHostToDevice), "copy type_id");
+    ICC_CUDA(cudaMemcpyAsync(d_type_id, type_id, (size_t)nel * 4, cudaMemcpyHostToDevice, stream), "copy type_id");
     host_type_id.assign(type_id, type_id + nel);
     for (int d = 0; d < 3; ++d) {
         host_type1d[d] = s.type1d[d];
@@ -350,9 +350,12 @@ int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type
     if ((rc = dev_alloc(&d_tile_start, tstart.size(), "alloc tiles"))) return rc;
     if ((rc = dev_alloc(&d_tile_type, ttype.size(), "alloc tiles"))) return rc;
     if ((rc = dev_alloc(&d_tile_elem, telem.size(), "alloc tiles"))) return rc;
-    ICC_CUDA(cudaMemcpy(d_tile_start, tstart.data(), tstart.size() * 4, cudaMemcpyHostToDevice), "copy tiles");
-    ICC_CUDA(cudaMemcpy(d_tile_type, ttype.data(), ttype.size() * 4, cudaMemcpyHostToDevice), "copy tiles");
-    ICC_CUDA(cudaMemcpy(d_tile_elem, telem.data(), telem.size(), cudaMemcpyHostToDevice), "copy tiles");
+    ICC_CUDA(cudaMemcpyAsync(d_tile_start, tstart.data(), tstart.size() * 4, cudaMemcpyHostToDevice, stream), "copy tiles");
+    ICC_CUDA(cudaMemcpyAsync(d_tile_type, ttype.data(), ttype.size() * 4, cudaMemcpyHostToDevice, stream), "copy tiles");
+    ICC_CUDA(cudaMemcpyAsync(d_tile_elem, telem.data(), telem.size(), cudaMemcpyHostToDevice, stream), "copy tiles");
+    // every set-up copy is ordered on the handle's stream (a non-blocking stream is not ordered
+    // after copies on the legacy default stream); the host arrays must outlive them
+    ICC_CUDA(cudaStreamSynchronize(stream), "set-up copies");
 
     if ((rc = dev_alloc(&d_scale, (size_t)nel, "alloc scale"))) return rc;
     if ((rc = dev_alloc(&d_mask, (size_t)ndof, "alloc mask"))) return rc;
@@ -363,7 +366,8 @@ int Op::init(const Space &s, const double *ke_types, int nt, const int32_t *type
     if ((rc = dev_alloc(&d_partials, (size_t)vec_blocks * 2, "alloc partials"))) return rc;
     if ((rc = dev_alloc(&d_state, 1, "alloc state"))) return rc;
     if ((rc = dev_alloc(&d_counter, 1, "alloc counter"))) return rc;
-    ICC_CUDA(cudaMemset(d_counter, 0, sizeof(unsigned)), "clear counter");
+    ICC_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned), stream), "clear counter");
+    ICC_CUDA(cudaStreamSynchronize(stream), "clear counter");
     ICC_CUDA(cudaMallocHost((void **)&h_state, sizeof(PcgState)), "alloc pinned state");
     ICC_CUDA(cudaFuncSetAttribute(apply_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kApplySmem),
              "cudaFuncSetAttribute");

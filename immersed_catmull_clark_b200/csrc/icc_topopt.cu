@@ -256,8 +256,10 @@ static int state_ktypes(Op &o, StateScratch &s) {
     if (s.ktypes) return ICC_OK;
     int rc;
     if ((rc = dalloc(&s.ktypes, o.host_ktypes.size(), "alloc element matrices"))) return rc;
-    ICC_CUDA(cudaMemcpy(s.ktypes, o.host_ktypes.data(), o.host_ktypes.size() * 8, cudaMemcpyHostToDevice),
+    ICC_CUDA(cudaMemcpyAsync(s.ktypes, o.host_ktypes.data(), o.host_ktypes.size() * 8, cudaMemcpyHostToDevice,
+                             o.stream),
              "copy element matrices");
+    ICC_CUDA(cudaStreamSynchronize(o.stream), "copy element matrices");
     return ICC_OK;
 }
 
@@ -440,9 +442,12 @@ int icc_topopt_create(const int64_t nel[3], const icc_topopt_cfg *cfg, icc_topop
         delete t;
         return rc;
     }
-    cudaMemcpy(t->d_force, force.data(), n * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(t->d_w, w.data(), w.size() * 8, cudaMemcpyHostToDevice);
-    cudaError_t e = cudaMemcpy(t->d_off, off.data(), off.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    // ordered on the operator's stream, which runs every later kernel of the loop
+    cudaError_t e = cudaMemcpyAsync(t->d_force, force.data(), n * 8, cudaMemcpyHostToDevice, o.stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t->d_w, w.data(), w.size() * 8, cudaMemcpyHostToDevice, o.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(t->d_off, off.data(), off.size() * sizeof(int4), cudaMemcpyHostToDevice, o.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(o.stream);
     if (e != cudaSuccess) {
         delete t;
         return icc::cuda_fail(e, "copy topopt set-up");
@@ -465,7 +470,8 @@ int icc_topopt_set_loads(icc_topopt *t, int32_t nload, const double *forces) {
         cudaFree(f);
         return rc;
     }
-    cudaError_t e = cudaMemcpy(f, forces, cnt * 8, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(f, forces, cnt * 8, cudaMemcpyHostToDevice, o.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(o.stream);
     if (e != cudaSuccess) {
         cudaFree(f);
         cudaFree(u);
