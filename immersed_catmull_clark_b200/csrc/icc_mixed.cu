@@ -554,12 +554,11 @@ __device__ bool grid_sync(unsigned long long *ctr, int *err) {
         const unsigned long long old = atomicAdd(ctr, 1ull);
         const unsigned long long target = (old / gridDim.x + 1ull) * gridDim.x;
         int ok = 0;
-        for (long long i = 0; i < kGridWaitLimit; ++i) {
+        for (long long i = 0; i < kGridWaitLimit; ++i) {   // each poll is an L2 round trip
             if (*(volatile unsigned long long *)ctr >= target) {
                 ok = 1;
                 break;
             }
-            __nanosleep(64);
         }
         if (!ok) atomicExch(err, 2);
         __threadfence();
@@ -591,8 +590,11 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const uint8_t *__restri
     const long long n = 3 * g.nsc;
     // 1. Ap at every node: its <= 8 brick partials in a fixed order, then the output rule
     double dot = 0.0;
+    // 32-bit index arithmetic: the set-up checks nsc < 2^31
+    const unsigned ucx = (unsigned)g.cx, ucy = (unsigned)g.cy;
     for (long long nd = t0; nd < g.nsc; nd += T) {
-        const int ix = int(nd % g.cx), iy = int((nd / g.cx) % g.cy), iz = int(nd / ((long long)g.cx * g.cy));
+        const unsigned u = (unsigned)nd, q1 = u / ucx;
+        const int ix = int(u - q1 * ucx), iy = int(q1 % ucy), iz = int(q1 / ucy);
         int bx[2], lx[2], by[2], ly[2], bz[2], lz[2];
         const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
         const int nby = node_bricks(iy, kBY, g.nby, by, ly);
@@ -834,6 +836,7 @@ static int setup_xform(const Op &op, Xform &xf) {
 
 static int mixed_init(Op &op) {
     if (op.mixed && op.mixed->ready) return ICC_OK;
+    if (op.g.nsc >= (1LL << 31)) return set_error(ICC_BAD_ARG, "tensor-core path: more than 2^31 control points");
     if (!op.mixed) op.mixed = new MixedState();
     MixedState &ms = *op.mixed;
     const int mt = setup_xform(op, ms.xf);
