@@ -512,14 +512,6 @@ __global__ void ir_to_f32_kernel(long long n, const double *__restrict__ r, floa
         r32[i] = float(r[i] * inv);
 }
 
-// x += |r| d
-__global__ void ir_update_kernel(long long n, double *__restrict__ x, const float *__restrict__ d,
-                                 const double *__restrict__ scalars) {
-    const double nr = sqrt(scalars[0]);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        x[i] += nr * double(d[i]);
-}
-
 // r = b - y; partial r'r
 __global__ void __launch_bounds__(kVecThreads)
 ir_residual_kernel(long long n, const double *__restrict__ b, const double *__restrict__ y, double *__restrict__ r,

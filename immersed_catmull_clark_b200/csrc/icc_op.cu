@@ -216,26 +216,6 @@ pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, dou
     }
 }
 
-__global__ void __launch_bounds__(kVecThreads) pcg_alpha_kernel(const double *__restrict__ partials, int np, PcgState *st) {
-    if (st->status != 0) return;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
-    s = block_sum(s);
-    if (threadIdx.x == 0) pcg_alpha_step(st, s);
-}
-
-__global__ void __launch_bounds__(kVecThreads) pcg_beta_kernel(const double *__restrict__ partials, int np, PcgState *st) {
-    if (st->status != 0) return;
-    double rr = 0.0, rz = 0.0;
-    for (int i = threadIdx.x; i < np; i += blockDim.x) {
-        rr += partials[2 * i];
-        rz += partials[2 * i + 1];
-    }
-    rr = block_sum(rr);
-    rz = block_sum(rz);
-    if (threadIdx.x == 0) pcg_beta_step(st, rr, rz);
-}
-
 // ------------------------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------------------------
