@@ -322,6 +322,18 @@ def run_topopt(args, wl):
     print(json.dumps(out), flush=True)
 
 
+def aggregate_replicas(dist, torch, device, t_ms, work, e2e_value):
+    """Replicas on N GPUs: the job's time is the slowest rank's (max over ranks), its throughput
+    the work of all ranks over that time; e2e throughputs add.  Returns (t_ms, value, e2e)."""
+    t = torch.tensor([t_ms, work, e2e_value], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    t_all = float(mx[0])
+    return t_all, float(sm[1]) / (t_all * 1e-3), float(sm[2])
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -496,11 +508,7 @@ def run_ours(args):
 
     # max over ranks of time, sum of throughput
     if world > 1:
-        tt = torch.tensor([t_ms, local_value, e2e_local], dtype=torch.float64, device=dev)
-        mx = tt.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = tt.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        t_ms_all = float(mx[0]); value = n * float(np.sum(iters)) * world / (t_ms_all * 1e-3)
-        e2e_value = float(sm[2])
+        t_ms_all, value, e2e_value = aggregate_replicas(dist, torch, dev, t_ms, n * float(np.sum(iters)), e2e_local)
     else:
         t_ms_all, value, e2e_value = t_ms, local_value, e2e_local
 
