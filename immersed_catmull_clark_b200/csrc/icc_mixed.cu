@@ -983,7 +983,8 @@ int mixed_apply_f32(Op &op, const float *x, float *y) {
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, op.mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "tc apply");
-    if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
+    if (err) return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
+                                                    : "tensor-core apply: mbarrier wait ran out");
     return ICC_OK;
 }
 
@@ -1016,7 +1017,8 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
-    if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
+    if (err) return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
+                                                    : "tensor-core apply: mbarrier wait ran out");
     *contract_ms = a / reps;
     *gather_ms = gt / reps;
     return ICC_OK;
@@ -1205,7 +1207,8 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
-    if (err) return set_error(ICC_TIMEOUT, "tensor-core apply: mbarrier wait ran out");
+    if (err) return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
+                                                    : "tensor-core apply: mbarrier wait ran out");
     ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
     *iters = ms.h_state->iter;
     *rel_res = res;

@@ -665,6 +665,12 @@ int icc_pcg_solve_batched(int32_t count, icc_op *const *ops, const double *const
         return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: null argument");
     for (int32_t i = 0; i < count; ++i)
         if (!ops[i] || !b[i] || !x[i]) return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: null instance argument");
+    {
+        std::vector<const icc_op *> seen(ops, ops + count);
+        std::sort(seen.begin(), seen.end());
+        if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
+            return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: a handle appears twice (each instance needs its own)");
+    }
     // instances on worker threads, each solving on its handle's own stream: the GPU interleaves the
     // instances' kernels (small grids leave SMs to the others); every solve is deterministic, so the
     // results equal those of sequential calls
