@@ -62,7 +62,6 @@ energies_kernel(Geom g, const double *__restrict__ K, const int *__restrict__ ty
 }
 
 // ---- deterministic reductions -------------------------------------------------------------------
-// kind 0: sum, 1: max
 __device__ __forceinline__ double block_max(double v) {
     __shared__ double wm[32];
 #pragma unroll
@@ -79,6 +78,7 @@ __device__ __forceinline__ double block_max(double v) {
     return r;
 }
 
+// part[0 .. np) -> *out, kind 0: sum, 1: max (fixed order)
 __global__ void __launch_bounds__(kTopoThreads) finish_kernel(const double *__restrict__ part, int np, int kind,
                                                               double *__restrict__ out) {
     double v = 0.0;
