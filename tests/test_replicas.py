@@ -34,7 +34,7 @@ def _worker(rank, world, port, out):
 
 def test_replica_aggregation_two_ranks():
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
