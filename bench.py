@@ -13,9 +13,12 @@ value    = DOF * iterations / device seconds of the solve, inputs resident in HB
 e2e      = the same metric through the host-pointer C ABI call (icc_op_update_scale +
            icc_pcg_solve): H2D of the step's scale and load, D2H of the solution, inside the timing.
 roofline = the dominant kernel: for the mixed form the tensor-core brick apply, algorithmic
-           3 * 2*81*81 flops per element (three split-TF32 products) over its mean CUDA-event
-           duration against this run's cuBLAS TF32 GEMM; for --mode fp64 the FP64 DMMA brick apply,
-           2*81*81 flops per element against this run's cuBLAS DGEMM.
+           2*81*81 flops per element (the three split-TF32 products are credited once) over its
+           mean CUDA-event duration against this run's cuBLAS TF32 GEMM (the MMA work it executes,
+           three products padded to 96 x 96, is reported beside it as executed_flops); for
+           --mode fp64 the FP64 DMMA brick apply, 2*81*81 flops per element against this run's
+           cuBLAS DGEMM.  roofline.iteration: the whole PCG iteration against HBM bandwidth,
+           algorithmic bytes per iteration over ms_per_step / iterations.
 cpu_baseline / --impl reference = the oracle (C restatement of the reference's CPU path:
            element-loop operator with OpenMP, serial PCG vector loops) on the host cores, a
            bounded number of PCG iterations of the same workload.
@@ -56,6 +59,28 @@ def make_problem(W, wl, seed):
     if wl.get("kind") == "cylinders":
         return W.cylinders(wl["n"])
     return W.cantilever(wl["nel"], smooth=wl["smooth"], seed=seed)
+
+
+def workload_label(prob, wl):
+    """The workload name both arms print (the same inputs: make_problem with the same seed)."""
+    if wl.get("kind") == "cylinders":
+        return f"{prob.name} immersed cube minus three cylinders"
+    return f"{prob.name} SIMP cantilever, " + ("smoothed densities" if wl.get("smooth") else "i.i.d. densities")
+
+
+def hbm_peak():
+    """HBM bandwidth denominator (GB/s): MEASURED_PEAKS.json's copy bandwidth when present, else the
+    pool's earlier measurement (6,650 GB/s)."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        for k in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if k in d and float(d[k]) > 0:
+                return float(d[k]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        pass
+    return 6650.0, "fallback 6,650 GB/s (MEASURED_PEAKS.json absent)"
 
 
 def parse():
@@ -167,9 +192,36 @@ def gemm_peak(torch, dev, dtype, tf32=False):
     return best
 
 
-def cpu_sample(problem, seconds, oracle_mod):
-    """Oracle (reference CPU path restated in C) PCG iterations on the host for ~seconds."""
+def cpu_sample_csr(problem, oracle_mod):
+    """The reference's own CPU path, restated in C by the oracle: AssemblyPattern CSR assembly
+    (rust/src/sparse.rs:128-175), then Jacobi-PCG to 1e-8 with the row-parallel CSR SpMV
+    (rust/src/sparse.rs:60-68) inside the masked closure (rust/src/topopt_iga.rs:151-159)."""
     O = oracle_mod
+    osp = O.Space(problem.bounds, problem.nel, 2)
+    lam, mu = O.lame(1.0, 0.3)
+    types, tid, _ = osp.element_matrices(lam, mu)
+    b = np.where(problem.free_mask > 0, problem.force, 0.0)
+    t0 = time.perf_counter()
+    k = O.Csr.assemble(osp, types, tid, problem.scale)
+    t_asm = time.perf_counter() - t0
+    diag = np.maximum(k.diagonal(), 1e-12)
+    t0 = time.perf_counter()
+    x, it, res = k.pcg(b, diag, 20 * problem.ndof, TOL, problem.free_mask, 1)
+    dt = time.perf_counter() - t0
+    return {"value": problem.ndof * it / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"full solve of {problem.name} ({problem.ndof} DOF) to {TOL:g}: CSR assembly "
+                      f"{t_asm * 1e3:.1f} ms (not in value), Jacobi-PCG {it} iterations {dt * 1e3:.1f} ms with the "
+                      f"row-parallel CSR SpMV (OpenMP) and serial vector loops",
+            "seconds": dt, "assembly_ms": t_asm * 1e3, "iterations": it}
+
+
+def cpu_sample(problem, seconds, oracle_mod):
+    """Oracle (reference CPU path restated in C) PCG iterations on the host for ~seconds.  The small
+    cantilever (19,656 DOF) runs the reference's assembled path to convergence; larger problems, whose
+    CSR does not fit in host memory, run a bounded number of iterations of the matrix-free element loop."""
+    O = oracle_mod
+    if problem.ndof <= 200000:
+        return cpu_sample_csr(problem, O)
     osp = O.Space(problem.bounds, problem.nel, 2)
     lam, mu = O.lame(1.0, 0.3)
     types, tid, _ = osp.element_matrices(lam, mu)
@@ -208,7 +260,7 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-           "config": {"workload": prob.name, "ndof": prob.ndof, "tol": TOL, "seed": SEED},
+           "config": {"workload": workload_label(prob, wl), "ndof": prob.ndof, "tol": TOL, "seed": SEED},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[0]["cores"], "kind": "port",
                             "sample": vals[0]["sample"]},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -222,12 +274,10 @@ def run_batched(args, wl):
     import immersed_catmull_clark_b200 as icc
     from immersed_catmull_clark_b200 import workloads as W
 
-    rng = np.random.default_rng(SEED)
-    ks = rng.integers(wl["kmin"], wl["kmax"] + 1, size=wl["count"])
+    ks, probs = W.batched_designs(wl["count"], wl["kmin"], wl["kmax"], SEED)
     lam, mu = icc.lame(W.E0, W.NU)
     ops, bs, ndofs = [], [], []
-    for i, k in enumerate(ks):
-        p = W.cantilever((2 * int(k), int(k), int(k)), seed=SEED + 1 + i)
+    for p in probs:
         sp = icc.SpaceBox(p.bounds, p.nel, 2)
         em = icc.elasticity_element_matrices(sp, lam, mu)
         ops.append(icc.MatrixFreeOperator(sp, em, p.scale, p.free_mask, icc.MASK_ZERO))
@@ -446,11 +496,15 @@ def run_ours(args):
 
     # roofline of the dominant kernel, timed on the solver's stream
     flops_el = 2.0 * 81 * 81
+    nbricks = int(np.prod([-(-d // b) for d, b in zip(sp.nel_dir, (8, 4, 4))]))
+    executed = None
     if precision == icc.MIXED:
         y32 = torch.empty(n, dtype=torch.float32, device=dev)
         p32 = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev).to(torch.float32)
         contract_ms, gather_ms = op.profile_apply_f32(p32.data_ptr(), y32.data_ptr(), 20)
-        flops = 3.0 * flops_el * sp.nel   # the three split-TF32 products of every element
+        flops = flops_el * sp.nel   # algorithmic: one 81 x 81 product per element
+        # executed MMA work: three split products of 128 x 96 x 96 per brick of 8 x 4 x 4 elements
+        executed = 3 * 2.0 * 128 * 96 * 96 * nbricks
         peak = gemm_peak(torch, dev, torch.float32, tf32=True)
         kname, tkey = "apply_tc_kernel (tcgen05 kind::tf32, 3-term split)", "apply_tc_kernel"
         peak_src = ("measured in this run: cuBLAS TF32 GEMM (torch.matmul float32 with TF32 tensor cores, 8192^3); "
@@ -460,19 +514,29 @@ def run_ours(args):
         p_dev = torch.from_numpy(np.random.default_rng(1).standard_normal(n)).to(dev)
         contract_ms, gather_ms = op.profile_apply(p_dev.data_ptr(), y_dev.data_ptr(), 20)
         flops = flops_el * sp.nel
+        executed = 2.0 * 88 * 84 * sp.nel   # DMMA tiles: 81 padded to 84 (trial) x 88 (test)
         peak = gemm_peak(torch, dev, torch.float64)
         kname, tkey = "apply_f64_kernel (FP64 DMMA)", "apply_f64_kernel"
         peak_src = ("measured in this run: cuBLAS DGEMM (torch.matmul float64 8192^3); "
                     "MEASURED_PEAKS.json has no FP64 figure")
     achieved = flops / (contract_ms * 1e-3) / 1e12
-    traffic = None
+    traffic, traffic_src = None, None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         try:
             t = json.load(open(tpath)).get(tkey, {}).get(args.workload)
             traffic = None if t is None else float(t)
+            traffic_src = ("dram__bytes_read.sum + dram__bytes_write.sum of one launch from an earlier ncu capture "
+                           "of the same kernel and workload, recorded in profiles/ncu_traffic.json (not this run)")
         except Exception:
             traffic = None
+    # the whole iteration against HBM: the apply reads p and s_e and writes Ap, the vector step
+    # reads x, r, p, Ap, D^-1 and writes x, r, p (FP32 for the mixed form, FP64 for the plain one)
+    vb = 4 if precision == icc.MIXED else 8
+    iter_bytes = 5 * vb * n + vb * sp.nel + 3 * vb * n
+    ms_per_iter = float(np.sum(ms_steps)) / max(1, int(np.sum(iters)))
+    hbm, hbm_src = hbm_peak()
+    iter_gbs = iter_bytes / (ms_per_iter * 1e-3) / 1e9
 
     # end to end through the host-pointer C ABI call (pinned host buffers)
     b_pin = torch.from_numpy(b_host).pin_memory()
@@ -520,7 +584,7 @@ def run_ours(args):
         cpu.pop("seconds", None)
 
     if rank == 0:
-        cfg = {"workload": f"{prob.name} SIMP cantilever, smoothed densities" if wl.get("smooth") else prob.name,
+        cfg = {"workload": workload_label(prob, wl),
                "ndof": n, "nel": sp.nel, "tol": TOL, "seed": SEED, "mode": args.mode,
                "iterations": iters, "time_to_tol_ms": ms_steps,
                "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"}
@@ -531,9 +595,14 @@ def run_ours(args):
                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == icc.FP64 else "tf32x3+f32+f64",
                "data": "synthetic", "config": cfg,
                "roofline": {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak,
-                            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
-                            "algorithmic_flops_per_launch": flops, "launch_ms": contract_ms,
-                            "node_sum_kernel_ms": gather_ms, "peak_source": peak_src},
+                            "unit": "TFLOP/s", "frac": achieved / peak, "frac_of": "measured", "traffic": traffic,
+                            "traffic_source": traffic_src,
+                            "algorithmic_flops_per_launch": flops, "executed_flops_per_launch": executed,
+                            "executed_tflops": executed / (contract_ms * 1e-3) / 1e12,
+                            "launch_ms": contract_ms, "node_sum_kernel_ms": gather_ms, "peak_source": peak_src,
+                            "iteration": {"bound": "hbm", "algorithmic_bytes": iter_bytes, "ms": ms_per_iter,
+                                          "achieved_gbs": iter_gbs, "peak_gbs": hbm, "frac": iter_gbs / hbm,
+                                          "peak_source": hbm_src}},
                "cpu_baseline": cpu,
                "e2e": {"value": e2e_value, "unit": UNIT,
                        "h2d_bytes_per_step": 8 * n + 8 * sp.nel + (8 * n if diag_host is not None else 0),

@@ -46,7 +46,7 @@ EXPORTED = [
     "icc_op_profile_apply_f32", "icc_solve_state", "icc_op_element_energies", "icc_topopt_create",
     "icc_topopt_destroy", "icc_topopt_run", "icc_cylinder_weights", "icc_pcg_solve_batched",
     "icc_topopt_set_loads",
-    "icc_apply_f64_noalloc",
+    "icc_apply_f64_noalloc", "icc_op_set_wait_limit",
 ]
 
 
@@ -118,6 +118,7 @@ def lib():
     L.icc_op_profile_apply.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.icc_op_profile_apply_f32.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.icc_apply_f64_noalloc.argtypes = [i64p, vp, i32, vp, vp, vp, vp, vp]
+    L.icc_op_set_wait_limit.argtypes = [vp, i64]
     L.icc_solve_state.argtypes = [vp, f64p, f64p, i64, dbl, C.POINTER(SolveOpts), f64p, C.POINTER(i64),
                                   C.POINTER(dbl)]
     L.icc_op_element_energies.argtypes = [vp, f64p, i64, f64p, i64]
@@ -278,6 +279,10 @@ class MatrixFreeOperator:
         _check(lib().icc_op_element_energies(self._h, np.ascontiguousarray(u, dtype=np.float64), self.n, ee,
                                              self.sp.nel))
         return ee
+
+    def set_wait_limit(self, grid_polls):
+        """Polls of a grid barrier in the mixed solve's fused vector step before ICC_TIMEOUT."""
+        _check(lib().icc_op_set_wait_limit(self._h, int(grid_polls)))
 
     def last_solve_info(self):
         info = SolveInfo()

@@ -109,6 +109,7 @@ void state_release(Op &op);
 int mixed_on_scale_update(Op &op);
 int mixed_apply_f32(Op &op, const float *x, float *y);
 int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms);
+int mixed_set_wait_limit(Op &op, long long polls);
 int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter,
                 const icc_solve_opts &opts, double *x, int64_t *iters, double *rel_res);
 

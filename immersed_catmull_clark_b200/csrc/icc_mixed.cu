@@ -45,6 +45,7 @@ constexpr int kBFl = kTcN * kTcK;      // floats per B term
 constexpr uint32_t kBLbo = (kTcN / 8) * 128;  // bytes between K-adjacent core matrices of B
 constexpr uint32_t kSbo = 128;                // bytes between 8-row groups
 constexpr long long kWaitLimit = 1LL << 22;
+constexpr long long kGridWaitLimit = 1LL << 22;   // default polls of a grid barrier before it gives up
 
 // offset (floats) of element (row, k) in the canonical K-major no-swizzle layout with `rows` rows
 __host__ __device__ __forceinline__ int canon(int row, int k, int rows) {
@@ -81,10 +82,13 @@ struct MixedState {
     double *d_tail_part = nullptr;            // [3][tail_grid] partial sums of the fused vector step
     unsigned long long *d_grid_ctr = nullptr;  // grid barrier counter of the fused vector step
     int tail_grid = 0;
+    long long grid_wait_limit = kGridWaitLimit;
+    int *h_err = nullptr;                      // pinned copy of d_err read after every graph batch
     PcgState *d_state = nullptr, *h_state = nullptr;
     double *h_scalars = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_batch = 0;
+    long long graph_limit = 0;   // grid_wait_limit the graph was captured with
 };
 
 // ------------------------------------------------------------------------------------------
@@ -104,9 +108,12 @@ struct MixedState {
 //   warps 12-23 (epilogue, same split): read their 32 accumulator columns with tcgen05.ld and
 //     release them, apply R and sum the element results per patch node with warp shuffles (x, y)
 //     and a shared buffer (z), then write the brick partials.
-// mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full.
-// Every wait is bounded; on time-out the CTA raises a shared abort flag, so all roles finish
-// promptly and the host reports ICC_TIMEOUT.
+// mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full, fin.
+// Every wait is bounded.  On time-out the waiting thread raises a shared abort flag; every other
+// wait then returns false at once.  The builders and the epilogue decide at a barrier that ORs
+// the flag over the role, so all threads of a role leave their loop at the same brick; the MMA
+// thread stops issuing, then commits once more and waits (bounded) for that commit, so no MMA
+// of the CTA is in flight when TMEM is released.  The host reports ICC_TIMEOUT.
 constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24
 constexpr int kRoleThreads = kRoleWarps * 32;
 constexpr int kPtThreads = (2 * kRoleWarps + 1) * 32;
@@ -206,11 +213,12 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
     float *sP = sAlo + 2 * kAloFl;        // [3][3 * kPVol] input patches
     float *sZb = sP + 3 * 3 * kPVol;      // [2][kZFl] per-layer node partials, by brick parity
-    __shared__ __align__(8) uint64_t bars[9];
+    __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
     __shared__ float s_r[3][5][9];
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8;
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
+             *fin = bars + 9;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
@@ -228,6 +236,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         tc::mbar_init(&d_empty[0], kRoleThreads);
         tc::mbar_init(&d_empty[1], kRoleThreads);
         tc::mbar_init(b_full, 1);
+        tc::mbar_init(fin, 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
@@ -300,8 +309,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const float vm = valid ? se : 0.f;
             tc::cp_async_wait<2>();
-            tc::named_sync(1, kRoleThreads);   // brick it's patch has landed for every builder
-            if (it >= 2) pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
+            const bool ok = it < 2 || pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
+            // brick it's patch has landed for every builder; all builders leave together on abort
+            if (tc::named_sync_or(1, kRoleThreads, !ok || s_abort != 0)) break;
             tc::fence_after_sync();
             const float *Pc = sP + pb * 3 * kPVol + base;
             float v[27];
@@ -374,7 +384,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             const BrickBox bb = we.box(g);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const int db = it & 1;
-            pt_wait(&d_full[db], uint32_t(it >> 1) & 1u, &s_abort, err);
+            // on a failed wait the values read below are not used: the barrier before the z-sum
+            // makes every epilogue thread leave the loop
+            const bool ok = pt_wait(&d_full[db], uint32_t(it >> 1) & 1u, &s_abort, err);
             tc::fence_after_sync();
             uint32_t dv[32];
             tc::tmem_ld32(dcol0 + (uint32_t)(db * kTcN), dv);
@@ -424,7 +436,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
                 }
             // all layers of brick it are in sZ[it & 1]; every z-sum of brick it - 1 (which read
             // the other buffer) finished before its thread reached this barrier
-            tc::named_sync(2, kRoleThreads);
+            if (tc::named_sync_or(2, kRoleThreads, !ok || s_abort != 0)) break;
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
             float *ob = patch_out + (size_t)b * 3 * kPVol + et;
 #pragma unroll
@@ -442,16 +454,19 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         constexpr uint32_t idesc = tc::idesc_tf32(kTcM, kTcN);
         tc::mbar_arrive_expect_tx(b_full, kBBytes);
         tc::bulk_g2s(sB, bmat, kBBytes, b_full);
-        pt_wait(b_full, 0u, &s_abort, err);
+        const bool b_ok = pt_wait(b_full, 0u, &s_abort, err);
+        bool run = b_ok;
         // descriptors of K step 0 (hi and lo terms); the shared-memory window is below 256 KB,
         // so adding a step's offset never carries out of the address field
         const uint64_t dbh0 = tc::make_desc(sB, kBLbo, kSbo), dbl0 = tc::make_desc(sB + kBFl, kBLbo, kSbo);
         const uint64_t dal0 = tc::make_desc(sAlo, kALbo, kSbo), dal1 = tc::make_desc(sAlo + kAloFl, kALbo, kSbo);
-        for (int it = 0; it < nmine; ++it) {
+        for (int it = 0; it < nmine && run; ++it) {
             const int s = it & 1, db = it & 1;
-            pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err);
-            // brick it - 2 has been drained from accumulator buffer db
-            if (it >= 2) pt_wait(&d_empty[db], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
+            // slot s holds brick it, and brick it - 2 has been drained from accumulator buffer db;
+            // on a failed wait nothing more is issued
+            run = pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err) &&
+                  (it < 2 || pt_wait(&d_empty[db], uint32_t((it >> 1) - 1) & 1u, &s_abort, err));
+            if (!run) break;
             tc::fence_after_sync();
             const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
             const uint32_t dacc = tmem + (uint32_t)(kColD + db * kTcN);
@@ -469,8 +484,14 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             tc::mma_commit(&d_full[db]);
             tc::mma_commit(&a_empty[s]);
         }
-        for (int it = nmine - 2; it < nmine; ++it)
-            if (it >= 0) pt_wait(&d_empty[it & 1], uint32_t(it >> 1) & 1u, &s_abort, err);
+        if (run)
+            for (int it = nmine - 2; it < nmine; ++it)
+                if (it >= 0 && !pt_wait(&d_empty[it & 1], uint32_t(it >> 1) & 1u, &s_abort, err)) break;
+        // every MMA this thread issued has completed once fin arrives; then TMEM may be released.
+        // A B copy whose wait failed is waited for again, so it does not land after the CTA ends.
+        tc::mma_commit(fin);
+        tc::mbar_wait_bounded(fin, 0u, kWaitLimit);
+        if (!b_ok) tc::mbar_wait_bounded(b_full, 0u, kWaitLimit);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -533,12 +554,12 @@ __global__ void to_f32_kernel(long long n, const double *__restrict__ a, float *
 
 // ---- fused vector step of the FP32 recurrence ------------------------------------------------
 constexpr int kTailThreads = 256;
-constexpr long long kGridWaitLimit = 1LL << 22;
 
-// Grid-wide barrier of a cooperative launch (every CTA resident).  The counter only grows; a CTA
-// waits for the next multiple of gridDim.x above its own arrival.  Bounded: false on time-out
-// (err set), so a stuck barrier ends the kernel instead of hanging the GPU.
-__device__ bool grid_sync(unsigned long long *ctr, int *err) {
+// Grid-wide barrier of a cooperative launch (every CTA resident).  The counter only grows (the
+// host clears it before each solve); a CTA waits for the next multiple of gridDim.x above its own
+// arrival.  Bounded by `limit` polls: false on time-out (err = 2), so a stuck barrier ends the
+// kernel instead of hanging the GPU.
+__device__ bool grid_sync(unsigned long long *ctr, int *err, long long limit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -546,7 +567,7 @@ __device__ bool grid_sync(unsigned long long *ctr, int *err) {
         const unsigned long long old = atomicAdd(ctr, 1ull);
         const unsigned long long target = (old / gridDim.x + 1ull) * gridDim.x;
         int ok = 0;
-        for (long long i = 0; i < kGridWaitLimit; ++i) {   // each poll is an L2 round trip
+        for (long long i = 0; i < limit; ++i) {   // each poll is an L2 round trip
             if (*(volatile unsigned long long *)ctr >= target) {
                 ok = 1;
                 break;
@@ -570,7 +591,7 @@ __global__ void __launch_bounds__(kTailThreads)
 pcg_tail_kernel(Geom g, const float *__restrict__ patch, const uint8_t *__restrict__ mask, int mask_mode,
                 const float *__restrict__ inv, float *__restrict__ x, float *__restrict__ r, float *__restrict__ p,
                 float *__restrict__ pm, float *__restrict__ ap, double *__restrict__ part, PcgState *st,
-                unsigned long long *ctr, int *err) {
+                unsigned long long *ctr, int *err, long long wait_limit) {
     __shared__ PcgState S;
     __shared__ int s_stat;
     __shared__ double s_coef;
@@ -614,7 +635,7 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const uint8_t *__restri
     }
     dot = block_sum(dot);
     if (threadIdx.x == 0) part[blockIdx.x] = dot;
-    if (!grid_sync(ctr, err)) return;
+    if (!grid_sync(ctr, err, wait_limit)) return;
     // 2. alpha
     double pap = 0.0;
     for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) pap += __ldcg(part + i);
@@ -643,7 +664,7 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const uint8_t *__restri
         part[gridDim.x + 2 * blockIdx.x] = rr;
         part[gridDim.x + 2 * blockIdx.x + 1] = rz;
     }
-    if (!grid_sync(ctr, err)) return;
+    if (!grid_sync(ctr, err, wait_limit)) return;
     // 4. convergence test and beta, or a request for a residual replacement
     double a = 0.0, c = 0.0;
     for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
@@ -892,6 +913,7 @@ static int mixed_init(Op &op) {
     if ((rc = dalloc(&ms.d_state, 1, "alloc mixed"))) return rc;
     ICC_CUDA(cudaMallocHost((void **)&ms.h_state, sizeof(PcgState)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&ms.h_scalars, 8 * sizeof(double)), "alloc pinned");
+    ICC_CUDA(cudaMallocHost((void **)&ms.h_err, sizeof(int)), "alloc pinned");
     ICC_CUDA(cudaMemsetAsync(ms.d_err, 0, sizeof(int), op.stream), "clear err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "clear err");
     ICC_CUDA(cudaFuncSetAttribute(apply_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPtSmem),
@@ -911,6 +933,7 @@ void mixed_release(Op &op) {
         if (p) cudaFree(p);
     if (ms.h_state) cudaFreeHost(ms.h_state);
     if (ms.h_scalars) cudaFreeHost(ms.h_scalars);
+    if (ms.h_err) cudaFreeHost(ms.h_err);
     delete op.mixed;
     op.mixed = nullptr;
 }
@@ -971,20 +994,43 @@ static cudaError_t enqueue_inner_iteration(Op &op) {
     return cudaLaunchKernelEx(&cfg, pcg_tail_kernel, op.g, (const float *)ms.d_patch32,
                               (const uint8_t *)(zero || ident ? op.d_mask : nullptr), op.mask_mode,
                               (const float *)ms.d_inv32, ms.d_x32, ms.d_r32, ms.d_p32, ident ? ms.d_xm32 : nullptr,
-                              ms.d_ap32, ms.d_tail_part, ms.d_state, ms.d_grid_ctr, ms.d_err);
+                              ms.d_ap32, ms.d_tail_part, ms.d_state, ms.d_grid_ctr, ms.d_err,
+                              ms.grid_wait_limit);
+}
+
+// Clears the device error flag and the grid-barrier counter before a call, so a handle whose
+// previous call timed out starts clean (stream-ordered before the call's kernels).
+static int clear_flags(Op &op) {
+    MixedState &ms = *op.mixed;
+    ICC_CUDA(cudaMemsetAsync(ms.d_err, 0, sizeof(int), op.stream), "clear err");
+    ICC_CUDA(cudaMemsetAsync(ms.d_grid_ctr, 0, sizeof(unsigned long long), op.stream), "clear grid counter");
+    return ICC_OK;
+}
+
+static int timeout_error(int err) {
+    return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
+                                           : "tensor-core apply: mbarrier wait ran out");
 }
 
 // y32 = A x32 on the tensor cores (icc_op_apply_f32).
 int mixed_apply_f32(Op &op, const float *x, float *y) {
     int rc = mixed_init(op);
     if (rc) return rc;
+    if ((rc = clear_flags(op))) return rc;
     enqueue_apply_tc(op, x, y);
     ICC_CUDA(cudaGetLastError(), "tc apply launch");
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, op.mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "tc apply");
-    if (err) return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
-                                                    : "tensor-core apply: mbarrier wait ran out");
+    if (err) return timeout_error(err);
+    return ICC_OK;
+}
+
+// Polls of a grid barrier before the fused vector step gives up (ICC_TIMEOUT).
+int mixed_set_wait_limit(Op &op, long long polls) {
+    int rc = mixed_init(op);
+    if (rc) return rc;
+    op.mixed->grid_wait_limit = polls;
     return ICC_OK;
 }
 
@@ -992,6 +1038,7 @@ int mixed_apply_f32(Op &op, const float *x, float *y) {
 int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms) {
     int rc = mixed_init(op);
     if (rc) return rc;
+    if ((rc = clear_flags(op))) return rc;
     MixedState &ms = *op.mixed;
     std::vector<cudaEvent_t> ev(3 * size_t(reps));
     for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
@@ -1017,8 +1064,7 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
-    if (err) return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
-                                                    : "tensor-core apply: mbarrier wait ran out");
+    if (err) return timeout_error(err);
     *contract_ms = a / reps;
     *gather_ms = gt / reps;
     return ICC_OK;
@@ -1081,6 +1127,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     int rc = op.ensure_pcg_buffers();
     if (rc) return rc;
     if ((rc = mixed_init(op))) return rc;
+    if ((rc = clear_flags(op))) return rc;
     MixedState &ms = *op.mixed;
     const int vb = op.vec_blocks;
     const long long n = op.ndof;
@@ -1123,7 +1170,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         launches++;
     }
 
-    if (!ms.graph || ms.graph_batch != check_every) {
+    if (!ms.graph || ms.graph_batch != check_every || ms.graph_limit != ms.grid_wait_limit) {
         if (ms.graph) cudaGraphExecDestroy(ms.graph);
         ms.graph = nullptr;
         cudaGraph_t graph;
@@ -1137,6 +1184,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         cudaGraphDestroy(graph);
         ICC_CUDA(e, "graph instantiate");
         ms.graph_batch = check_every;
+        ms.graph_limit = ms.grid_wait_limit;
     }
 
     int status = ICC_NOT_CONVERGED;
@@ -1151,7 +1199,9 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
         launches += 2 * int64_t(check_every);
         launched += check_every;
         ICC_CUDA(cudaMemcpyAsync(ms.h_state, ms.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, op.stream), "state");
+        ICC_CUDA(cudaMemcpyAsync(ms.h_err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
         ICC_CUDA(cudaStreamSynchronize(op.stream), "inner sync");
+        if (*ms.h_err) return timeout_error(*ms.h_err);   // a bounded wait ran out in this batch
         const PcgState hs = *ms.h_state;
         // the device state asks for a residual replacement when the FP32 recurrence has gained
         // delta or after a bounded segment (an FP32 recurrence stalls once its drift from the true
@@ -1207,8 +1257,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     int err = 0;
     ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
-    if (err) return set_error(ICC_TIMEOUT, err == 2 ? "fused vector step: grid barrier wait ran out"
-                                                    : "tensor-core apply: mbarrier wait ran out");
+    if (err) return timeout_error(err);
     ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
     *iters = ms.h_state->iter;
     *rel_res = res;

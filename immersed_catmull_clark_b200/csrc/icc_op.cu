@@ -743,6 +743,12 @@ int icc_op_profile_apply_f32(icc_op *op, const float *x_dev, float *y_dev, int32
     return icc::mixed_profile_apply(op->op, x_dev, y_dev, reps, contract_ms, gather_ms);
 }
 
+int icc_op_set_wait_limit(icc_op *op, int64_t grid_polls) {
+    if (!op || grid_polls < 0) return set_error(ICC_BAD_ARG, "icc_op_set_wait_limit: bad argument");
+    cudaSetDevice(op->op.device);
+    return icc::mixed_set_wait_limit(op->op, grid_polls);
+}
+
 int icc_op_last_solve_info(const icc_op *op, icc_solve_info *info) {
     if (!op || !info) return set_error(ICC_BAD_ARG, "icc_op_last_solve_info: null argument");
     *info = op->op.last_info;

@@ -175,6 +175,21 @@ __device__ __forceinline__ void named_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// named barrier among `count` threads that also returns the OR of `pred` over all of them, so the
+// threads of a role take the same branch after it (used to leave a loop together on abort)
+__device__ __forceinline__ bool named_sync_or(int id, int count, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
+}
+
 // round to TF32 (10 explicit mantissa bits), nearest, ties away from zero
 __device__ __forceinline__ float to_tf32(float v) {
     uint32_t r;

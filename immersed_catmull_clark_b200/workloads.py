@@ -237,3 +237,12 @@ def reference_tip_load(nel):
     f = np.zeros(3 * nsc)
     f[nsc + idx[sel]] = -1.0 / sel.sum()
     return f
+
+
+def batched_designs(count=64, kmin=8, kmax=48, seed=2026):
+    """The batched-designs configuration: `count` cantilever designs of 2k x k x k elements with
+    k ~ U{kmin..kmax} drawn from the seed, design i with its own densities (seed + 1 + i).
+    Returns (ks, problems)."""
+    rng = np.random.default_rng(seed)
+    ks = rng.integers(kmin, kmax + 1, size=count)
+    return ks, [cantilever((2 * int(k), int(k), int(k)), seed=seed + 1 + i) for i, k in enumerate(ks)]

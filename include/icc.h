@@ -221,6 +221,12 @@ int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t
 int icc_op_profile_apply_f32(icc_op *op, const float *x_dev, float *y_dev, int32_t reps, double *contract_ms,
                              double *gather_ms);
 
+/* Polls of a grid-wide barrier in the mixed solve's fused vector step before it gives up and the
+ * solve returns ICC_TIMEOUT (default 2^22).  The error flag and the barrier counter are cleared at
+ * the start of every call, so the handle works normally after a time-out.  Lets a test make the
+ * bounded wait run out without a fault; no reference counterpart. */
+int icc_op_set_wait_limit(icc_op *op, int64_t grid_polls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -934,9 +934,12 @@ void orc_solve_state(const orc_csr *k, const uint8_t *free_mask, const double *f
 
 /* rust/src/topopt_iga.rs:73-234 CantileverTopOpt::{new, run}.  cfg = [size0, size1, size2,
  * volfrac, penal, rmin, young, poisson, emin, move_limit, pcg_tol]; nel[3]; max_iter.
+ * nload > 0 replaces the reference's single tip load by nload load cases (forces[nload * ndof]):
+ * each case keeps its own warm-started state, the compliance is |sum_k F_k'u_k| and the element
+ * energies are summed over the cases (the reference loop is the case nload = 1).
  * Outputs: compliance[max_iter] (per iteration), density[nel]; returns iterations run. */
-int orc_topopt_run(const int *nel, const double *cfg, int max_iter, double *compliance_out,
-                   double *density_out, i64 *pcg_iters_out) {
+int orc_topopt_run_loads(const int *nel, const double *cfg, int max_iter, int nload_cases, const double *forces,
+                         double *compliance_out, double *density_out, i64 *pcg_iters_out) {
     double bounds[6] = {0.0, cfg[0], 0.0, cfg[1], 0.0, cfg[2]};
     double volfrac = cfg[3], penal = cfg[4], rmin = cfg[5], young = cfg[6], poisson = cfg[7];
     double emin = cfg[8], move = cfg[9], pcg_tol = cfg[10];
@@ -962,6 +965,8 @@ int orc_topopt_run(const int *nel, const double *cfg, int max_iter, double *comp
         if (i1 == nd[0] && fabs(i2 - 1.0) <= 1.0 && fabs(i3 - (double)nd[2] / 2.0) <= 1.0) load[nload++] = i;
     }
     for (i64 k = 0; k < nload; k++) force[sp->ndof_sc + load[k]] = -1.0 / (double)nload;
+    int ncase = nload_cases > 0 ? nload_cases : 1;
+    const double *fcase = nload_cases > 0 ? forces : force;
     /* sensitivity filter (rust/src/topopt_iga.rs:94-120) */
     double h[3];
     for (int d = 0; d < 3; d++) h[d] = sp->lengths[d] / (double)sp->nel_dir[d];
@@ -1002,7 +1007,7 @@ int orc_topopt_run(const int *nel, const double *cfg, int max_iter, double *comp
     double *ee = (double *)malloc(sizeof(double) * (size_t)ne);
     double *dc_raw = (double *)malloc(sizeof(double) * (size_t)ne);
     double *dc = (double *)malloc(sizeof(double) * (size_t)ne);
-    double *u = (double *)calloc((size_t)n, sizeof(double));
+    double *u_all = (double *)calloc((size_t)n * (size_t)ncase, sizeof(double));
     double *un = (double *)malloc(sizeof(double) * (size_t)n);
     for (i64 e = 0; e < ne; e++) x[e] = volfrac;
     int done = 0;
@@ -1010,24 +1015,33 @@ int orc_topopt_run(const int *nel, const double *cfg, int max_iter, double *comp
         memcpy(x_old, x, sizeof(double) * (size_t)ne);
         for (i64 e = 0; e < ne; e++) scale[e] = emin + (1.0 - emin) * pow(x[e], penal);
         orc_csr *k = orc_assemble_pattern(n, sp->connectivity, 81, ne, types, type_id, scale);
-        i64 it; double res;
-        orc_solve_state(k, free_mask, force, u, pcg_tol, un, &it, &res);
-        orc_csr_free(k);
-        memcpy(u, un, sizeof(double) * (size_t)n);
+        i64 it = 0;
         double c = 0.0;
-        for (i64 i = 0; i < n; i++) c += force[i] * u[i];
-        /* element_energies (topopt_iga.rs:165-184) */
-        for (i64 e = 0; e < ne; e++) {
-            const double *ke = types + (size_t)type_id[e] * 81 * 81;
-            const i64 *ce = sp->connectivity + e * 81;
-            double sm = 0.0;
-            for (int a = 0; a < 81; a++) {
-                double ua = u[ce[a]], row = 0.0;
-                for (int b = 0; b < 81; b++) row += ke[a * 81 + b] * u[ce[b]];
-                sm += ua * row;
+        for (i64 e = 0; e < ne; e++) ee[e] = 0.0;
+        for (int q = 0; q < ncase; q++) {
+            const double *fq = fcase + (size_t)q * (size_t)n;
+            double *u = u_all + (size_t)q * (size_t)n;
+            i64 itq; double res;
+            orc_solve_state(k, free_mask, fq, u, pcg_tol, un, &itq, &res);
+            it += itq;
+            memcpy(u, un, sizeof(double) * (size_t)n);
+            double cq = 0.0;
+            for (i64 i = 0; i < n; i++) cq += fq[i] * u[i];
+            c += cq;
+            /* element_energies (topopt_iga.rs:165-184), summed over the cases */
+            for (i64 e = 0; e < ne; e++) {
+                const double *ke = types + (size_t)type_id[e] * 81 * 81;
+                const i64 *ce = sp->connectivity + e * 81;
+                double sm = 0.0;
+                for (int a = 0; a < 81; a++) {
+                    double ua = u[ce[a]], row = 0.0;
+                    for (int b = 0; b < 81; b++) row += ke[a * 81 + b] * u[ce[b]];
+                    sm += ua * row;
+                }
+                ee[e] += sm;
             }
-            ee[e] = sm;
         }
+        orc_csr_free(k);
         for (i64 e = 0; e < ne; e++) dc_raw[e] = -penal * (1.0 - emin) * pow(x[e], penal - 1.0) * ee[e];
         for (i64 e = 0; e < ne; e++) {
             double sm = 0.0;
@@ -1058,11 +1072,16 @@ int orc_topopt_run(const int *nel, const double *cfg, int max_iter, double *comp
         if (change < 0.01 && iter >= 15) break;
     }
     memcpy(density_out, x, sizeof(double) * (size_t)ne);
-    free(x); free(x_old); free(cand); free(scale); free(ee); free(dc_raw); free(dc); free(u); free(un);
+    free(x); free(x_old); free(cand); free(scale); free(ee); free(dc_raw); free(dc); free(u_all); free(un);
     free(cen); free(fptr); free(fidx); free(fw); free(fsum);
     free(types); free(type_id); free(free_mask); free(force); free(load);
     orc_space_free(sp);
     return done;
+}
+
+int orc_topopt_run(const int *nel, const double *cfg, int max_iter, double *compliance_out,
+                   double *density_out, i64 *pcg_iters_out) {
+    return orc_topopt_run_loads(nel, cfg, max_iter, 0, NULL, compliance_out, density_out, pcg_iters_out);
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -76,6 +76,8 @@ def lib():
                                       C.POINTER(C.c_double)]
         L.orc_topopt_run.argtypes = [i32p, f64p, C.c_int, f64p, f64p, i64p]
         L.orc_topopt_run.restype = C.c_int
+        L.orc_topopt_run_loads.argtypes = [i32p, f64p, C.c_int, C.c_int, vp, f64p, f64p, i64p]
+        L.orc_topopt_run_loads.restype = C.c_int
         L.orc_element_weights.argtypes = [f64p, i64p, C.c_int64, f64p, i32p, i32p, f64p, i8p]
         L.orc_cylinders_weights.argtypes = [i32p, i32p, C.c_double, f64p, i8p]
         L.orc_legacy_stabilization.argtypes = [vp, i8p, C.c_double, vp, vp, vp]
@@ -273,15 +275,22 @@ def pcg_mf(sp, types, type_id, scale, b, diag, max_iter, tol, free_mask=None, ma
 
 
 def topopt_run(nel, volfrac, penal, rmin, max_iter, pcg_tol, size=(1.2, 0.6, 0.3), young=1.0,
-               poisson=0.3, emin=1e-3, move_limit=0.2):
-    """rust/src/topopt_iga.rs:187-234 CantileverTopOpt::run with CantileverTopOptConfig."""
+               poisson=0.3, emin=1e-3, move_limit=0.2, loads=None):
+    """rust/src/topopt_iga.rs:187-234 CantileverTopOpt::run with CantileverTopOptConfig.  loads
+    (nload x ndof) replaces the single tip load by load cases: compliance |sum_k F_k'u_k| and the
+    element energies summed over the cases, each case warm-started from its own previous state."""
     cfg = np.array([size[0], size[1], size[2], volfrac, penal, rmin, young, poisson, emin,
                     move_limit, pcg_tol])
     comp = np.zeros(max_iter)
     ne = int(np.prod(nel))
     dens = np.zeros(ne)
     its = np.zeros(max_iter, dtype=np.int64)
-    n = lib().orc_topopt_run(np.asarray(nel, dtype=np.int32), cfg, max_iter, comp, dens, its)
+    if loads is None:
+        n = lib().orc_topopt_run(np.asarray(nel, dtype=np.int32), cfg, max_iter, comp, dens, its)
+    else:
+        f = np.ascontiguousarray(np.atleast_2d(loads), dtype=np.float64)
+        n = lib().orc_topopt_run_loads(np.asarray(nel, dtype=np.int32), cfg, max_iter, f.shape[0],
+                                       f.ctypes.data_as(C.c_void_p), comp, dens, its)
     return comp[:n], dens, its[:n]
 
 
