@@ -46,7 +46,8 @@ EXPORTED = [
     "icc_op_profile_apply_f32", "icc_solve_state", "icc_op_element_energies", "icc_topopt_create",
     "icc_topopt_destroy", "icc_topopt_run", "icc_cylinder_weights", "icc_pcg_solve_batched",
     "icc_topopt_set_loads",
-    "icc_apply_f64_noalloc", "icc_op_set_wait_limit",
+    "icc_apply_f64_noalloc", "icc_op_set_wait_limit", "icc_op_set_extra_triplets", "icc_ghost_penalty",
+    "icc_legacy_stabilization",
 ]
 
 
@@ -119,6 +120,9 @@ def lib():
     L.icc_op_profile_apply_f32.argtypes = [vp, vp, vp, i32, C.POINTER(dbl), C.POINTER(dbl)]
     L.icc_apply_f64_noalloc.argtypes = [i64p, vp, i32, vp, vp, vp, vp, vp]
     L.icc_op_set_wait_limit.argtypes = [vp, i64]
+    L.icc_op_set_extra_triplets.argtypes = [vp, i64, vp, vp, vp]
+    L.icc_ghost_penalty.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, i64, C.POINTER(i64)]
+    L.icc_legacy_stabilization.argtypes = [vp, vp, dbl, vp, vp, vp, i64, C.POINTER(i64)]
     L.icc_solve_state.argtypes = [vp, f64p, f64p, i64, dbl, C.POINTER(SolveOpts), f64p, C.POINTER(i64),
                                   C.POINTER(dbl)]
     L.icc_op_element_energies.argtypes = [vp, f64p, i64, f64p, i64]
@@ -231,6 +235,17 @@ class MatrixFreeOperator:
     def update_scale(self, scale):
         s = None if scale is None else np.ascontiguousarray(scale, dtype=np.float64)
         _check(lib().icc_op_update_scale(self._h, _vp(s)))
+
+    def set_extra_triplets(self, rows, cols, vals):
+        """Adds the sparse term S (triplets, duplicates summed) to the operator: y = mask rule of
+        (K + S)(m .* x), the stabilised closures of rust/src/topopt_immersed.rs:174-183 and
+        rust/src/immersed.rs:558-566.  Empty triplets remove it."""
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        c = np.ascontiguousarray(cols, dtype=np.int64)
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        if not (len(r) == len(c) == len(v)):
+            raise ValueError("rows, cols and vals must have the same length")
+        _check(lib().icc_op_set_extra_triplets(self._h, len(v), _vp(r), _vp(c), _vp(v)))
 
     def update_mask(self, free_mask, mask_mode):
         fm = None if free_mask is None else np.ascontiguousarray(free_mask, dtype=np.uint8)
@@ -391,6 +406,29 @@ class CantileverTopOpt:
         _check(lib().icc_topopt_run(self._h, max_iter, _vp(comp), _vp(chg), _vp(its), _vp(dens), C.byref(done)))
         k = done.value
         return TopOptHistory(comp[:k], chg[:k], its[:k], dens)
+
+
+def _triplets(fn, *args):
+    cnt = C.c_int64()
+    _check(fn(*args, None, None, None, 0, C.byref(cnt)))
+    n = cnt.value
+    r = np.zeros(n, dtype=np.int64)
+    c = np.zeros(n, dtype=np.int64)
+    v = np.zeros(n)
+    _check(fn(*args, _vp(r), _vp(c), _vp(v), n, C.byref(cnt)))
+    return r, c, v
+
+
+def ghost_penalty(sp, status, gamma, young):
+    """Face ghost penalty of the immersed solve (rust/src/immersed.rs:224-370) as triplets."""
+    st = np.ascontiguousarray(status, dtype=np.int8)
+    return _triplets(lib().icc_ghost_penalty, sp._h, _vp(st), float(gamma), float(young))
+
+
+def legacy_stabilization(sp, status, gamma):
+    """The reference's legacy cut-cell springs (rust/src/immersed.rs:156-222) as triplets."""
+    st = np.ascontiguousarray(status, dtype=np.int8)
+    return _triplets(lib().icc_legacy_stabilization, sp._h, _vp(st), float(gamma))
 
 
 def cylinder_weights(res, sub, radius):

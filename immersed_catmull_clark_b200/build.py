@@ -10,7 +10,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libicc.so")
-SOURCES = ["icc_op.cu", "icc_mixed.cu", "icc_topopt.cu", "icc_immersed.cu", "icc_noalloc.cu", "icc_space.cpp"]
+SOURCES = ["icc_op.cu", "icc_mixed.cu", "icc_topopt.cu", "icc_immersed.cu", "icc_noalloc.cu", "icc_space.cpp", "icc_stab.cpp"]
 HEADERS = ["icc_internal.h", "icc_device.cuh", "icc_vec.cuh", "icc_tc.cuh"]
 
 NVCC_FLAGS = [

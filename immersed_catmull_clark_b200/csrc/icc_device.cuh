@@ -45,13 +45,42 @@ struct PcgState {
     double rz_old, p_ap, alpha, beta, norm_b, rel_res, tol;
     double rz_prev;        // r'z used by the last alpha (the beta of a residual replacement needs it)
     long long iter, max_iter;
-    int status, pad;
+    int status;
+    int fresh;             // mixed form: rz_old and rr_old are exact (set at the start and at replacements)
     // mixed form: ask for a residual replacement once rel_res < repl_delta * repl_res or after
     // repl_seg iterations since iteration repl_iter (repl_delta = 0: never); the test runs every
     // repl_every iterations (the host's batch), which keeps replacements from coming too often
     double repl_res, repl_delta;
     long long repl_iter, repl_seg, repl_every;   // tested only when iter is a multiple of repl_every
+    double rr_old;         // mixed form: r'r of the current residual
 };
+
+// A sparse term S added to the operator: CSR with 32-bit row pointers and columns over the
+// operator's DOFs, values in the vector type of the path that reads it (FP64 or FP32).
+template <class T>
+struct Sparse {
+    const int *ptr = nullptr, *idx = nullptr;
+    const T *val = nullptr;
+};
+
+// Boundary extraction.  On open uniform knots the B-splines of every element are a fixed
+// recombination of the uniform (translated) quadratic B-splines: along each direction N = E B with
+// E the identity except on the first two and the last two control points (knot insertion at the
+// ends).  With K_u the element matrix of the uniform basis, which is the same for every element of
+// the grid, the operator is K = E (sum_e s_e P_e' K_u P_e) E' (E = E_z (x) E_y (x) E_x per
+// component).  The tensor-core apply therefore runs every element on K_u: its input patches are
+// transformed by E' on the boundary control planes, and the node sums by E in the node-side pass.
+struct Edge {
+    int nb[3];          // boundary control points of direction d with a non-identity E (0: E = I)
+    int id[3][4];       // their indices among 0, 1, n, n + 1
+    float e[3][4][4];   // e[d][a][b] = E[id a][id b]
+};
+
+__device__ __forceinline__ int edge_slot(const Edge &E, int d, int i) {
+    for (int a = 0; a < E.nb[d]; ++a)
+        if (E.id[d][a] == i) return a;
+    return -1;
+}
 
 struct MixedState;  // tensor-core path (icc_mixed.cu)
 struct StateScratch;  // warm-started state solve and element energies (icc_topopt.cu)
@@ -69,6 +98,21 @@ struct Op {
     int *d_type_id = nullptr, *d_tile_start = nullptr, *d_tile_type = nullptr;
     uint8_t *d_tile_elem = nullptr, *d_mask = nullptr;
     double *d_patch = nullptr;              // brick patch partial sums [nbricks][3][kPVol]
+    // extra sparse term (icc_op_set_extra_triplets): y = mask rule of (K + S)(m .* x)
+    int *d_sp_ptr = nullptr, *d_sp_idx = nullptr;
+    double *d_sp_val = nullptr, *d_sp_diag = nullptr;
+    float *d_sp_val32 = nullptr;
+    int64_t sp_nnz = 0;
+    Sparse<double> extra64() const {
+        Sparse<double> s;
+        if (sp_nnz) { s.ptr = d_sp_ptr; s.idx = d_sp_idx; s.val = d_sp_val; }
+        return s;
+    }
+    Sparse<float> extra32() const {
+        Sparse<float> s;
+        if (sp_nnz) { s.ptr = d_sp_ptr; s.idx = d_sp_idx; s.val = d_sp_val32; }
+        return s;
+    }
     double *d_x_in = nullptr, *d_y_out = nullptr;
     // PCG
     double *d_x = nullptr, *d_r = nullptr, *d_p = nullptr, *d_ap = nullptr, *d_inv = nullptr, *d_b = nullptr,
@@ -92,6 +136,7 @@ struct Op {
     int set_scale(const double *scale);
     int set_scale_dev(const double *scale_dev);   // device array, stream-ordered
     int set_mask(const uint8_t *free_mask, int mode);
+    int set_extra(int64_t count, const int64_t *rows, const int64_t *cols, const double *vals);
     void enqueue_apply(const double *x, double *y, double *partials, const PcgState *st);
     int apply_dev(const double *x, double *y);
     int diagonal_dev(double *d);
@@ -110,6 +155,7 @@ int mixed_on_scale_update(Op &op);
 int mixed_apply_f32(Op &op, const float *x, float *y);
 int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms);
 int mixed_set_wait_limit(Op &op, long long polls);
+void mixed_invalidate_graph(Op &op);
 int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter,
                 const icc_solve_opts &opts, double *x, int64_t *iters, double *rel_res);
 

@@ -20,8 +20,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -52,34 +54,19 @@ __host__ __device__ __forceinline__ int canon(int row, int k, int rows) {
     return (k >> 2) * (rows / 8) * 32 + (row >> 3) * 32 + (row & 7) * 4 + (k & 3);
 }
 
-// Class of an element position along one direction of n elements: on open uniform knots the two
-// first and the two last elements restrict the B-splines differently, all others alike.
-__host__ __device__ __forceinline__ int pos_class(int e, int n) {
-    const int r = n - 1 - e;
-    return r < 2 ? 4 - r : (e < 2 ? e : 2);
-}
-
-// Every element of a uniform grid spans the same quadratics, so its local basis is a fixed
-// 3x3 recombination of the most frequent element's along each direction: N_e = R_d N_main.
-// Then K_e = R K_main R^T with R = (R_z (x) R_y (x) R_x) per component, and one MMA pass with
-// K_main serves every element: the operand gets R^T u_e, the result R (K_main R^T u_e).
-struct Xform {
-    float r[3][5][9];    // R of each direction and position class, row-major
-    unsigned nonid[3];   // bit k: class k is not the identity
-};
-
 struct MixedState {
     bool ready = false;
-    float4 *d_bmat = nullptr;        // K_main split [hi, lo][kBFl] in the canonical layout
-    Xform xf{};
-    uint8_t *d_bflags = nullptr;     // per brick: bit d set when an element needs R along direction d
+    float4 *d_bmat = nullptr;        // K_u split [hi, lo][kBFl] in the canonical layout
+    Edge edge{};
+    Edge *d_edge = nullptr;          // the same in device memory, for the node-side passes
+    uint8_t *d_bflags = nullptr;     // per brick: bit d set when its patch holds boundary points of d
     float *d_scale32 = nullptr;
     float *d_patch32 = nullptr;
     float *d_rhs32 = nullptr, *d_x32 = nullptr, *d_r32 = nullptr, *d_p32 = nullptr, *d_ap32 = nullptr,
           *d_inv32 = nullptr, *d_xm32 = nullptr;   // xm32: masked input of the brick apply
     double *d_x64 = nullptr, *d_r64 = nullptr, *d_y64 = nullptr, *d_scalars = nullptr;
     int *d_err = nullptr;
-    double *d_tail_part = nullptr;            // [3][tail_grid] partial sums of the fused vector step
+    double *d_tail_part = nullptr;            // [7][tail_grid] partial sums of the fused vector step
     unsigned long long *d_grid_ctr = nullptr;  // grid barrier counter of the fused vector step
     int tail_grid = 0;
     long long grid_wait_limit = kGridWaitLimit;
@@ -173,25 +160,38 @@ struct BrickWalk {
     }
 };
 
-// v <- M v along direction D of a 27-vector v[az*9 + ay*3 + ax], M = R (TR false) or R^T (TR true)
-template <int D, bool TR>
-__device__ __forceinline__ void xform_dir(float (&v)[27], const float *R) {
-    float m[9];
+// V = E' u on the boundary control points of direction D inside the patch P (3 x kPZ x kPY x kPX,
+// patch origin o along D, ext of its control points inside the grid); line t along D (t < the
+// number of lines) is handled by thread t.  Every control point that a boundary value needs lies
+// in the patch: the set-up checks that E couples only control points of a common element.
+template <int D>
+__device__ __forceinline__ void edge_in(float *P, const Edge &E, int o, int ext, int t) {
+    constexpr int LA = D == 0 ? kPY : kPX;   // extent of the line index that runs fastest
+    constexpr int LB = D == 2 ? kPY : kPZ;
+    constexpr int stride = D == 0 ? 1 : (D == 1 ? kPX : kPX * kPY);
+    if (t >= 3 * LA * LB) return;
+    const int c = t / (LA * LB), w = t - c * (LA * LB), a1 = w % LA, a2 = w / LA;
+    const int base = D == 0 ? c * kPVol + (a2 * kPY + a1) * kPX
+                            : (D == 1 ? c * kPVol + a2 * (kPY * kPX) + a1 : c * kPVol + a2 * kPX + a1);
+    const int nb = E.nb[D];
+    float u[4], v[4];
+    int loc[4];
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int a = 0; a < 4; ++a) {
+        const int l = a < nb ? E.id[D][a] - o : -1;
+        loc[a] = (l >= 0 && l < ext) ? l : -1;
+        u[a] = loc[a] >= 0 ? P[base + loc[a] * stride] : 0.f;
+    }
 #pragma unroll
-        for (int j = 0; j < 3; ++j) m[3 * i + j] = TR ? R[3 * j + i] : R[3 * i + j];
-    constexpr int st = D == 0 ? 1 : (D == 1 ? 3 : 9);
+    for (int b = 0; b < 4; ++b) {
+        float acc = 0.f;
 #pragma unroll
-    for (int p = 0; p < 3; ++p)
+        for (int a = 0; a < 4; ++a) acc = fmaf(E.e[D][a][b], u[a], acc);
+        v[b] = acc;
+    }
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const int i0 = D == 0 ? p * 9 + q * 3 : (D == 1 ? p * 9 + q : p * 3 + q);
-            const float a = v[i0], b = v[i0 + st], c = v[i0 + 2 * st];
-            v[i0] = fmaf(m[2], c, fmaf(m[1], b, m[0] * a));
-            v[i0 + st] = fmaf(m[5], c, fmaf(m[4], b, m[3] * a));
-            v[i0 + 2 * st] = fmaf(m[8], c, fmaf(m[7], b, m[6] * a));
-        }
+    for (int b = 0; b < 4; ++b)
+        if (loc[b] >= 0) P[base + loc[b] * stride] = v[b];
 }
 
 __device__ __forceinline__ float row_scale(const Geom &g, const BrickBox &bb, int r, const float *__restrict__ scale) {
@@ -205,8 +205,8 @@ __device__ __forceinline__ float row_scale(const Geom &g, const BrickBox &bb, in
 // the compiler caps a thread at 72
 __global__ void __launch_bounds__(kPtThreads, 1)
 apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ scale, const float4 *__restrict__ bmat,
-                const Xform xf, const uint8_t *__restrict__ bflags, float *__restrict__ patch_out, int *__restrict__ err,
-                const PcgState *__restrict__ st) {
+                const Edge *__restrict__ edge, const uint8_t *__restrict__ bflags, float *__restrict__ patch_out,
+                int *__restrict__ err, const PcgState *__restrict__ st) {
     if (st && st->status != 0) return;
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
@@ -216,7 +216,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
-    __shared__ float s_r[3][5][9];
+    __shared__ Edge s_edge;
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
              *fin = bars + 9;
 
@@ -225,7 +225,8 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         tc::tmem_alloc(&tmem_base, kPtTmemCols);
         tc::tmem_relinquish();
     }
-    for (int i = tid; i < 3 * 5 * 9; i += kPtThreads) (&s_r[0][0][0])[i] = (&xf.r[0][0][0])[i];
+    for (int i = tid; i < int(sizeof(Edge) / 4); i += kPtThreads)
+        reinterpret_cast<int *>(&s_edge)[i] = reinterpret_cast<const int *>(edge)[i];
     if (tid == 0) {
         tc::mbar_init(&a_full[0], kRoleThreads);
         tc::mbar_init(&a_full[1], kRoleThreads);
@@ -295,7 +296,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         float se_next = nmine > 0 ? row_scale(g, wc.box(g), r, scale) : 0.f;
         for (int it = 0; it < nmine; ++it, wc.next(g), wl.next(g)) {
             const int s = it & 1, pb = it % 3;
-            const unsigned fl = fl_next;   // bit d: the brick needs R along direction d
+            const unsigned fl = fl_next;   // bit d: the brick's patch holds boundary points of d
             const float se = se_next;      // s_e of this thread's element (0 outside the grid)
             if (it + 1 < nmine) {
                 fl_next = bflags[blockIdx.x + (it + 1) * gridDim.x];
@@ -312,22 +313,34 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             const bool ok = it < 2 || pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
             // brick it's patch has landed for every builder; all builders leave together on abort
             if (tc::named_sync_or(1, kRoleThreads, !ok || s_abort != 0)) break;
+            if (fl) {   // V = E' u on the boundary control planes, one direction after the other
+                float *P = sP + pb * 3 * kPVol;
+                if (fl & 1u) {
+                    edge_in<0>(P, s_edge, bb.x0, min(kPX, g.cx - bb.x0), tid);
+                    tc::named_sync(1, kRoleThreads);
+                }
+                if (fl & 2u) {
+                    edge_in<1>(P, s_edge, bb.y0, min(kPY, g.cy - bb.y0), tid);
+                    tc::named_sync(1, kRoleThreads);
+                }
+                if (fl & 4u) {
+                    edge_in<2>(P, s_edge, bb.z0, min(kPZ, g.cz - bb.z0), tid);
+                    tc::named_sync(1, kRoleThreads);
+                }
+            }
             tc::fence_after_sync();
             const float *Pc = sP + pb * 3 * kPVol + base;
             float v[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) v[a] = Pc[(a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
-            // Element-local shift: K_e maps a constant per-component field to zero, so subtracting
+            // Element-local shift: K_u maps a constant per-component field to zero, so subtracting
             // the element's centre control value changes nothing in exact arithmetic while the
             // split operands carry only the variation across the element; the TF32 splitting
             // error then scales with that variation instead of with |u| (smooth, low-energy
-            // vectors of a converging PCG).  R^T maps constants to themselves.
+            // vectors of a converging PCG).
             const float nctr = -v[13] * vm;
 #pragma unroll
             for (int a = 0; a < 27; ++a) v[a] = fmaf(v[a], vm, nctr);   // s_e (v - ctr), or 0 outside the grid
-            if (fl & 1u) xform_dir<0, true>(v, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
-            if (fl & 2u) xform_dir<1, true>(v, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
-            if (fl & 4u) xform_dir<2, true>(v, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
             // A_hi into TMEM (lane = element), A_lo into shared memory in the canonical layout
             const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(s * kColSlot + c * 32);
             float *alo = sAlo + s * kAloFl + canon(q * 32 + lane, c * 32, kTcM);
@@ -335,7 +348,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             for (int q8 = 0; q8 < 4; ++q8) {
                 float hi[8], lo[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) tc::split_tf32(q8 * 8 + j < 27 ? v[q8 * 8 + j] : 0.f, hi[j], lo[j]);
+                for (int j = 0; j < 8; ++j) tc::split_tf32_raw(q8 * 8 + j < 27 ? v[q8 * 8 + j] : 0.f, hi[j], lo[j]);
                 tc::tmem_st8(col + q8 * 8, hi);
                 // 4 consecutive k of one row are 16 contiguous bytes; k + 4 is one core-matrix column on
                 *reinterpret_cast<float4 *>(alo + (2 * q8) * (kTcM / 8) * 32) = make_float4(lo[0], lo[1], lo[2], lo[3]);
@@ -358,11 +371,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         const int lx = lane & 7, ly = lane >> 3;
         const uint32_t dcol0 = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kColD + c * 32);
         const unsigned FULL = 0xffffffffu;
-        BrickWalk we;
-        we.init(g, blockIdx.x, gridDim.x);
-        BrickWalk wn = we;
-        wn.next(g);
-        unsigned fl_next = nmine > 0 ? bflags[blockIdx.x] : 0u;
         // lane masks of the node sums as multipliers (FMA instead of selects)
         const float mx1 = lx >= 1 ? 1.f : 0.f, mx2 = lx >= 2 ? 1.f : 0.f;
         const float my1 = ly >= 1 ? 1.f : 0.f, my2 = ly >= 2 ? 1.f : 0.f;
@@ -377,12 +385,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             zb[k] = 9 * (kPY * kPX) * pz + (kPY * kPX) * ci + pyx;
             zpz[k] = pz;
         }
-        for (int it = 0; it < nmine; ++it, we.next(g), wn.next(g)) {
+        for (int it = 0; it < nmine; ++it) {
             const int b = blockIdx.x + it * gridDim.x;
-            const unsigned fl = fl_next;
             float *sZ = sZb + (it & 1) * kZFl;
-            const BrickBox bb = we.box(g);
-            const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const int db = it & 1;
             // on a failed wait the values read below are not used: the barrier before the z-sum
             // makes every epilogue thread leave the loop
@@ -393,13 +398,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             tc::tmem_wait_ld();
             tc::fence_before_sync();
             tc::mbar_arrive(&d_empty[db]);   // accumulator buffer db is free for brick it + 2
-            if (it + 1 < nmine) fl_next = bflags[b + gridDim.x];
             float res[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
-            if (fl & 1u) xform_dir<0, false>(res, s_r[0][valid ? pos_class(bb.x0 + lx, g.nx) : 2]);
-            if (fl & 2u) xform_dir<1, false>(res, s_r[1][valid ? pos_class(bb.y0 + ly, g.ny) : 2]);
-            if (fl & 4u) xform_dir<2, false>(res, s_r[2][valid ? pos_class(bb.z0 + q, g.nz) : 2]);
             // x, in place: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2) in res[o]; lanes
             // lx = 7 also carry px = 8 (v[1](7) + v[2](6)) in res[o+1] and px = 9 (v[2](7)) in res[o+2]
 #pragma unroll
@@ -581,119 +582,172 @@ __device__ bool grid_sync(unsigned long long *ctr, int *err, long long limit) {
     return s_ok != 0;
 }
 
-// One launch for everything of a PCG iteration after the operator (rust/src/solver.rs:38-71):
-// node sum of the brick partials with the output mask (Ap), p'Ap -> alpha, x += alpha p,
-// r -= alpha Ap, r'z and r'r -> convergence test and beta, p = z + beta p.  Every CTA reduces the
-// same partials in the same order, so all of them take the same branches; CTA 0 writes the state.
-// When the FP32 residual has gained the replacement factor (or the segment is long), the state
-// asks the host for an FP64 residual replacement and the direction update waits for it.
+// Deterministic block reduction of five values at once; the sums are valid in thread 0.
+__device__ __forceinline__ void block_sum5(double (&v)[5]) {
+    __shared__ double ws[5][kTailThreads / 32];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) ws[k][threadIdx.x >> 5] = v[k];
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            double r = threadIdx.x < (blockDim.x >> 5) ? ws[k][threadIdx.x] : 0.0;
+            v[k] = warp_sum(r);
+        }
+    }
+}
+
+// One launch for everything of a PCG iteration after the operator (rust/src/solver.rs:38-71),
+// with one grid-wide barrier.
+//   Phase A, node by node: Ap = the node sum of the brick partials (with the boundary extraction)
+//   plus the sparse term, output rule applied; and five dot products p'Ap, z'Ap, Ap'D^-1 Ap, r'Ap,
+//   Ap'Ap (z = D^-1 r).
+//   Barrier.  Every CTA reduces the same partials in the same order: alpha = r'z / p'Ap, and for
+//   r_new = r - alpha Ap, without another reduction,
+//       |r_new|^2 = r'r - 2 alpha r'Ap + alpha^2 Ap'Ap,
+//       r_new' D^-1 r_new = r'z - 2 alpha z'Ap + alpha^2 Ap'D^-1 Ap,
+//   which give the convergence test and beta = r_new'z_new / r'z.  When the FP32 residual has
+//   gained the replacement factor (or the segment is long) the state asks the host for an FP64
+//   residual replacement instead.
+//   Phase B: x += alpha p, r -= alpha Ap, p = D^-1 r + beta p (when the iteration goes on), and the
+//   exact r'r and r'z of the new r as per-CTA partials, which the next launch reduces in place of
+//   the formulas (so they bridge one iteration only).
+// CTA 0 writes the state.  All CTAs take the same branches.
 __global__ void __launch_bounds__(kTailThreads)
-pcg_tail_kernel(Geom g, const float *__restrict__ patch, const uint8_t *__restrict__ mask, int mask_mode,
-                const float *__restrict__ inv, float *__restrict__ x, float *__restrict__ r, float *__restrict__ p,
-                float *__restrict__ pm, float *__restrict__ ap, double *__restrict__ part, PcgState *st,
-                unsigned long long *ctr, int *err, long long wait_limit) {
+pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict__ edge, const uint8_t *__restrict__ mask,
+                int mask_mode, Sparse<float> sp, const float *__restrict__ inv, float *__restrict__ x,
+                float *__restrict__ r, float *__restrict__ p, float *__restrict__ pm, float *__restrict__ ap,
+                double *__restrict__ part, PcgState *st, unsigned long long *ctr, int *err, long long wait_limit) {
     __shared__ PcgState S;
+    __shared__ double s_ab[2];
     __shared__ int s_stat;
-    __shared__ double s_coef;
     if (threadIdx.x == 0) S = *st;
     __syncthreads();
     if (S.status != 0) return;
-    const long long T = (long long)gridDim.x * blockDim.x;
+    const int G = gridDim.x;
+    double *pa = part, *pb = part + 5 * G;   // phase A partials [5][G], exact r'r, r'z [2][G]
+    // exact r'r and r'z of the current r: from the state after an initialisation or replacement,
+    // else from the previous launch's phase B
+    double rr0 = S.rr_old, rz0 = S.rz_old;
+    if (!S.fresh) {
+        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int i = threadIdx.x; i < G; i += blockDim.x) {
+            v[0] += __ldcg(pb + i);
+            v[1] += __ldcg(pb + G + i);
+        }
+        block_sum5(v);
+        rr0 = v[0];
+        rz0 = v[1];
+    }
+    const long long T = (long long)G * blockDim.x;
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long n = 3 * g.nsc;
-    // 1. Ap at every node: its <= 8 brick partials in a fixed order, then the output rule
-    double dot = 0.0;
+    // A. Ap at every node and the five dot products
+    double dA[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const Edge *E = edge && (edge->nb[0] | edge->nb[1] | edge->nb[2]) ? edge : nullptr;
     // 32-bit index arithmetic: the set-up checks nsc < 2^31
     const unsigned ucx = (unsigned)g.cx, ucy = (unsigned)g.cy;
     for (long long nd = t0; nd < g.nsc; nd += T) {
         const unsigned u = (unsigned)nd, q1 = u / ucx;
         const int ix = int(u - q1 * ucx), iy = int(q1 % ucy), iz = int(q1 / ucy);
-        int bx[2], lx[2], by[2], ly[2], bz[2], lz[2];
-        const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
-        const int nby = node_bricks(iy, kBY, g.nby, by, ly);
-        const int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
-        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-        for (int a = 0; a < nbz; ++a)
-            for (int q = 0; q < nby; ++q)
-                for (int w = 0; w < nbx; ++w) {
-                    const size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
-                    const float *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
-                    s0 += pb[0];
-                    s1 += pb[kPVol];
-                    s2 += pb[2 * kPVol];
-                }
-        const float sv[3] = {s0, s1, s2};
+        float sv[3];
+        const int sx = E ? edge_slot(*E, 0, ix) : -1, sy = E ? edge_slot(*E, 1, iy) : -1,
+                  sz = E ? edge_slot(*E, 2, iz) : -1;
+        if (sx < 0 && sy < 0 && sz < 0) node_partials(g, patch, ix, iy, iz, sv[0], sv[1], sv[2]);
+        else edge_node(g, *E, patch, ix, iy, iz, sx, sy, sz, sv);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const long long idx = (long long)c * g.nsc + nd;
             float v = sv[c];
+            if (sp.ptr) v += sparse_row(sp, idx, p, mask, mask_mode);
             if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.f;
             else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
             ap[idx] = v;
-            dot += double(p[idx]) * double(v);
+            const float ri = r[idx], iv = inv[idx];
+            const double av = double(v);
+            dA[0] += double(p[idx]) * av;
+            dA[1] += double(iv * ri) * av;
+            dA[2] += double(iv * v) * av;
+            dA[3] += double(ri) * av;
+            dA[4] += av * av;
         }
     }
-    dot = block_sum(dot);
-    if (threadIdx.x == 0) part[blockIdx.x] = dot;
+    block_sum5(dA);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) pa[k * G + blockIdx.x] = dA[k];
     if (!grid_sync(ctr, err, wait_limit)) return;
-    // 2. alpha
-    double pap = 0.0;
-    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) pap += __ldcg(part + i);
-    pap = block_sum(pap);
-    if (threadIdx.x == 0) {
-        pcg_alpha_step(&S, pap);
-        s_stat = S.status;
-        s_coef = S.alpha;
-        if (S.status != 0 && blockIdx.x == 0) *st = S;
+    {
+        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int i = threadIdx.x; i < G; i += blockDim.x)
+#pragma unroll
+            for (int k = 0; k < 5; ++k) v[k] += __ldcg(pa + k * G + i);
+        block_sum5(v);
+        if (threadIdx.x == 0) {
+            // rust/src/solver.rs:41-51 (alpha or breakdown), :56-71 (residual test, beta)
+            S.iter += 1;
+            S.p_ap = v[0];
+            S.rz_prev = rz0;
+            S.fresh = 0;
+            if (!(v[0] > 0.0)) {
+                S.status = isfinite(v[0]) ? kStatBreakdown : kStatNan;
+            } else {
+                const double alpha = rz0 / v[0];
+                S.alpha = alpha;
+                const double rr1 = fmax(rr0 - 2.0 * alpha * v[3] + alpha * alpha * v[4], 0.0);
+                const double rz1 = rz0 - 2.0 * alpha * v[1] + alpha * alpha * v[2];
+                const double res = sqrt(rr1) / S.norm_b;
+                S.rel_res = res;
+                S.rr_old = rr1;
+                S.rz_old = rz1;
+                if (res < S.tol) S.status = kStatConverged;
+                else if (!isfinite(res) || !isfinite(rz1)) S.status = kStatNan;
+                else {
+                    S.beta = rz1 / rz0;
+                    if (S.iter >= S.max_iter) S.status = kStatMaxIter;
+                    else if (S.repl_delta > 0.0 && S.iter % S.repl_every == 0 &&
+                             (S.rel_res < S.repl_delta * S.repl_res || S.iter - S.repl_iter >= S.repl_seg))
+                        S.status = kStatReplace;
+                }
+            }
+            s_stat = S.status;
+            s_ab[0] = S.alpha;
+            s_ab[1] = S.beta;
+            if (blockIdx.x == 0) *st = S;
+        }
     }
     __syncthreads();
-    if (s_stat != 0) return;
-    // 3. x += alpha p, r -= alpha Ap; r'r and r'z
-    const float alpha = float(s_coef);
-    double rr = 0.0, rz = 0.0;
+    if (s_stat == kStatBreakdown || s_stat == kStatNan) return;
+    // B. x += alpha p, r -= alpha Ap; the direction only when the iteration goes on
+    const float alpha = float(s_ab[0]), beta = float(s_ab[1]);
+    const bool go = s_stat == 0;
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (long long i = t0; i < n; i += T) {
-        x[i] += alpha * p[i];
+        const float pi = p[i];
+        x[i] += alpha * pi;
         const float ri = r[i] - alpha * ap[i];
         r[i] = ri;
-        rr += double(ri) * double(ri);
-        rz += double(ri) * double(inv[i] * ri);
-    }
-    rr = block_sum(rr);
-    rz = block_sum(rz);
-    if (threadIdx.x == 0) {
-        part[gridDim.x + 2 * blockIdx.x] = rr;
-        part[gridDim.x + 2 * blockIdx.x + 1] = rz;
-    }
-    if (!grid_sync(ctr, err, wait_limit)) return;
-    // 4. convergence test and beta, or a request for a residual replacement
-    double a = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
-        a += __ldcg(part + gridDim.x + 2 * i);
-        c += __ldcg(part + gridDim.x + 2 * i + 1);
-    }
-    a = block_sum(a);
-    c = block_sum(c);
-    if (threadIdx.x == 0) {
-        pcg_beta_step(&S, a, c);
-        if (S.status == 0 && S.repl_delta > 0.0 && S.iter % S.repl_every == 0 &&
-            (S.rel_res < S.repl_delta * S.repl_res || S.iter - S.repl_iter >= S.repl_seg))
-            S.status = kStatReplace;
-        s_stat = S.status;
-        s_coef = S.beta;
-        if (blockIdx.x == 0) *st = S;
-    }
-    __syncthreads();
-    if (s_stat != 0) return;
-    // 5. p = D^-1 r + beta p, zero on fixed DOFs (ICC_MASK_ZERO) or with the masked copy pm
-    const float beta = float(s_coef);
-    for (long long i = t0; i < n; i += T) {
-        const float v = inv[i] * r[i] + beta * p[i];
-        if (pm) {
-            p[i] = v;
-            pm[i] = mask[i] ? v : 0.f;
-        } else {
-            p[i] = (mask && !mask[i]) ? 0.f : v;
+        const float zi = inv[i] * ri;
+        v[0] += double(ri) * double(ri);
+        v[1] += double(ri) * double(zi);
+        if (go) {
+            const float w = zi + beta * pi;
+            if (pm) {
+                p[i] = w;
+                pm[i] = mask[i] ? w : 0.f;
+            } else {
+                p[i] = (mask && !mask[i]) ? 0.f : w;
+            }
         }
+    }
+    block_sum5(v);
+    if (threadIdx.x == 0) {
+        pb[blockIdx.x] = v[0];
+        pb[G + blockIdx.x] = v[1];
     }
 }
 
@@ -760,12 +814,53 @@ static void apply_r3(const double *Rx, const double *Ry, const double *Rz, const
         }
 }
 
-// Single-pass set-up: the main (most frequent) element type, the 1-D transforms R of every
-// direction and position class, and the check that each element type's matrix equals
-// R K_main R^T (to 1e-9 of max |K_main|); returns the main type or -1 with the error set.
-static int setup_xform(const Op &op, Xform &xf) {
+// Values of the three uniform quadratic B-splines of an element at relative position t in [0, 1].
+static void uniform_basis(double t, double b[3]) {
+    b[0] = 0.5 * (1.0 - t) * (1.0 - t);
+    b[1] = 0.5 + t - t * t;
+    b[2] = 0.5 * t * t;
+}
+
+// Set-up of the tensor-core form:
+//  * R of every 1-D element type: its three local B-splines in terms of the uniform ones,
+//    N = R B, from the basis values at the element's three Gauss points;
+//  * K_u = R_m^-1 K_m R_m^-T from the most frequent element type m, and the check that every
+//    element type's matrix equals R K_u R' (to 1e-9 of max |K_u|);
+//  * E along each direction, assembled from the elements' R (E[e + a][e + b] = R_e[a][b]), with
+//    the checks that overlapping elements agree, that E differs from the identity only among the
+//    control points 0, 1, n, n + 1, and that E couples only control points of a common element
+//    (so a brick's patch holds what its boundary values need, and the transforms of single
+//    bricks add up to the global one).
+// Fills edge and kunif (81 x 81 row-major); ICC_BAD_ARG with the error set when the element
+// matrices are not of this form.
+static int setup_edge(const Op &op, Edge &edge, std::vector<double> &kunif) {
     const Geom &g = op.g;
     const int n[3] = {g.nx, g.ny, g.nz};
+    // R per direction and 1-D type
+    double xg[3] = {-std::sqrt(0.6), 0.0, std::sqrt(0.6)};
+    double vu[9], vuinv[9];
+    for (int q = 0; q < 3; ++q) {
+        double b[3];
+        uniform_basis(0.5 * (xg[q] + 1.0), b);
+        for (int i = 0; i < 3; ++i) vu[3 * i + q] = b[i];
+    }
+    if (!inv3(vu, vuinv)) return set_error(ICC_BAD_ARG, "tensor-core path: singular uniform basis");
+    std::vector<std::array<double, 9>> R1[3];
+    for (int d = 0; d < 3; ++d) {
+        if ((int)op.host_type1d[d].size() != n[d] || op.host_basis1d[d].empty())
+            return set_error(ICC_BAD_ARG, "tensor-core path: space without 1-D basis data");
+        for (const auto &vt : op.host_basis1d[d]) {
+            std::array<double, 9> r;
+            for (int i = 0; i < 3; ++i)
+                for (int b = 0; b < 3; ++b) {
+                    double acc = 0.0;
+                    for (int q = 0; q < 3; ++q) acc += vt[3 * i + q] * vuinv[3 * q + b];
+                    r[3 * i + b] = std::fabs(acc - (i == b ? 1.0 : 0.0)) < 1e-12 ? (i == b ? 1.0 : 0.0) : acc;
+                }
+            R1[d].push_back(r);
+        }
+    }
+    // K_u from the most frequent element type
     std::vector<long long> count((size_t)op.ntypes, 0);
     for (int32_t t : op.host_type_id) count[(size_t)t]++;
     int mt = 0;
@@ -774,77 +869,91 @@ static int setup_xform(const Op &op, Xform &xf) {
     long long e0 = 0;
     while (op.host_type_id[(size_t)e0] != mt) ++e0;
     const int pos0[3] = {int(e0 % g.nx), int((e0 / g.nx) % g.ny), int(e0 / ((long long)g.nx * g.ny))};
-    double R[3][5][9];
-    for (int d = 0; d < 3; ++d) {
-        const std::vector<int> &t1d = op.host_type1d[d];
-        if ((int)t1d.size() != n[d] || op.host_basis1d[d].empty()) {
-            set_error(ICC_BAD_ARG, "tensor-core path: space without 1-D basis data");
-            return -1;
-        }
-        const int main1d = t1d[(size_t)pos0[d]];
-        double vinv[9];
-        if (!inv3(op.host_basis1d[d][(size_t)main1d].data(), vinv)) {
-            set_error(ICC_BAD_ARG, "tensor-core path: singular 1-D basis");
-            return -1;
-        }
-        xf.nonid[d] = 0;
-        for (int k = 0; k < 5; ++k) {
-            int rep = -1;
-            for (int e = 0; e < n[d] && rep < 0; ++e)
-                if (pos_class(e, n[d]) == k) rep = e;
-            for (int i = 0; i < 9; ++i) R[d][k][i] = (i % 4 == 0) ? 1.0 : 0.0;
-            if (rep >= 0 && t1d[(size_t)rep] != main1d) {
-                const double *vt = op.host_basis1d[d][(size_t)t1d[(size_t)rep]].data();
-                for (int i = 0; i < 3; ++i)
-                    for (int b = 0; b < 3; ++b) {
-                        double s = 0.0;
-                        for (int q = 0; q < 3; ++q) s += vt[3 * i + q] * vinv[3 * q + b];
-                        R[d][k][3 * i + b] = s;
-                    }
-                // a split of numerically equal 1-D types is still the identity
-                double dev = 0.0;
-                for (int i = 0; i < 9; ++i) dev = std::fmax(dev, std::fabs(R[d][k][i] - ((i % 4 == 0) ? 1.0 : 0.0)));
-                if (dev > 1e-12) xf.nonid[d] |= 1u << k;
-                else
-                    for (int i = 0; i < 9; ++i) R[d][k][i] = (i % 4 == 0) ? 1.0 : 0.0;
-            }
-            for (int i = 0; i < 9; ++i) xf.r[d][k][i] = float(R[d][k][i]);
-        }
+    double Ri[3][9];
+    for (int d = 0; d < 3; ++d)
+        if (!inv3(R1[d][(size_t)op.host_type1d[d][(size_t)pos0[d]]].data(), Ri[d]))
+            return set_error(ICC_BAD_ARG, "tensor-core path: singular 1-D basis");
+    {
+        const double *Km = op.host_ktypes.data() + (size_t)mt * 81 * 81;
+        std::vector<double> t1(81 * 81);
+        kunif.assign(81 * 81, 0.0);
+        for (int j = 0; j < 81; ++j) apply_r3(Ri[0], Ri[1], Ri[2], Km + j, 81, t1.data() + j, 81);
+        for (int i = 0; i < 81; ++i) apply_r3(Ri[0], Ri[1], Ri[2], t1.data() + i * 81, 1, kunif.data() + i * 81, 1);
     }
-    // every element's matrix must be the transformed main matrix of its class triple (the 1-D
-    // grouping rounds matrices to 1e-12, so a class may hold several numerically equal types)
-    std::vector<char> seen((size_t)125 * op.ntypes, 0);
-    for (int ez = 0; ez < g.nz; ++ez)
-        for (int ey = 0; ey < g.ny; ++ey)
-            for (int ex = 0; ex < g.nx; ++ex) {
-                const int key = pos_class(ex, g.nx) + 5 * (pos_class(ey, g.ny) + 5 * pos_class(ez, g.nz));
-                const int t = op.host_type_id[(size_t)ex + (size_t)g.nx * ((size_t)ey + (size_t)g.ny * ez)];
-                seen[(size_t)key * op.ntypes + t] = 1;
-            }
-    const double *K0 = op.host_ktypes.data() + (size_t)mt * 81 * 81;
     double kmax = 0.0;
-    for (int i = 0; i < 81 * 81; ++i) kmax = std::fmax(kmax, std::fabs(K0[i]));
-    std::vector<double> t1(81 * 81), t2(81 * 81);
-    for (int key = 0; key < 125; ++key) {
-        bool any = false;
-        for (int t = 0; t < op.ntypes; ++t) any |= seen[(size_t)key * op.ntypes + t] != 0;
-        if (!any) continue;
-        const double *Rx = R[0][key % 5], *Ry = R[1][(key / 5) % 5], *Rz = R[2][key / 25];
-        for (int j = 0; j < 81; ++j) apply_r3(Rx, Ry, Rz, K0 + j, 81, t1.data() + j, 81);        // R K0
-        for (int i = 0; i < 81; ++i) apply_r3(Rx, Ry, Rz, t1.data() + i * 81, 1, t2.data() + i * 81, 1);  // (R K0) R^T
-        for (int t = 0; t < op.ntypes; ++t) {
-            if (!seen[(size_t)key * op.ntypes + t]) continue;
-            const double *Kt = op.host_ktypes.data() + (size_t)t * 81 * 81;
+    for (double v : kunif) kmax = std::fmax(kmax, std::fabs(v));
+    // every (element type, 1-D type triple) that occurs must be R K_u R'
+    {
+        std::vector<std::array<int, 4>> combos;
+        for (int ez = 0; ez < g.nz; ++ez)
+            for (int ey = 0; ey < g.ny; ++ey)
+                for (int ex = 0; ex < g.nx; ++ex) {
+                    const std::array<int, 4> k = {
+                        op.host_type_id[(size_t)ex + (size_t)g.nx * ((size_t)ey + (size_t)g.ny * ez)],
+                        op.host_type1d[0][(size_t)ex], op.host_type1d[1][(size_t)ey], op.host_type1d[2][(size_t)ez]};
+                    if (std::find(combos.begin(), combos.end(), k) == combos.end()) combos.push_back(k);
+                }
+        std::vector<double> t1(81 * 81), t2(81 * 81);
+        for (const auto &k : combos) {
+            const double *Rx = R1[0][(size_t)k[1]].data(), *Ry = R1[1][(size_t)k[2]].data(), *Rz = R1[2][(size_t)k[3]].data();
+            for (int j = 0; j < 81; ++j) apply_r3(Rx, Ry, Rz, kunif.data() + j, 81, t1.data() + j, 81);
+            for (int i = 0; i < 81; ++i) apply_r3(Rx, Ry, Rz, t1.data() + i * 81, 1, t2.data() + i * 81, 1);
+            const double *Kt = op.host_ktypes.data() + (size_t)k[0] * 81 * 81;
             double dmax = 0.0;
             for (int i = 0; i < 81 * 81; ++i) dmax = std::fmax(dmax, std::fabs(t2[(size_t)i] - Kt[i]));
-            if (!(dmax <= 1e-9 * kmax)) {
-                set_error(ICC_BAD_ARG, "tensor-core path: an element matrix is not the transformed main element "
-                                       "matrix (element matrices must come from the space's own bases)");
-                return -1;
+            if (!(dmax <= 1e-9 * kmax))
+                return set_error(ICC_BAD_ARG, "tensor-core path: an element matrix is not the uniform element matrix "
+                                              "seen through its B-spline basis (element matrices must come from the "
+                                              "space's own bases)");
+        }
+    }
+    // E per direction
+    std::memset(&edge, 0, sizeof(edge));
+    for (int d = 0; d < 3; ++d) {
+        const int nd = n[d];
+        std::map<std::pair<int, int>, double> E;
+        for (int e = 0; e < nd; ++e) {
+            const auto &r = R1[d][(size_t)op.host_type1d[d][(size_t)e]];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    const std::pair<int, int> key(e + a, e + b);
+                    const double v = r[(size_t)(3 * a + b)];
+                    auto it = E.find(key);
+                    if (it == E.end()) E.emplace(key, v);
+                    else if (std::fabs(it->second - v) > 1e-12 * std::fmax(1.0, std::fabs(v)))
+                        return set_error(ICC_BAD_ARG, "tensor-core path: element bases disagree on a shared B-spline");
+                }
+        }
+        std::vector<int> ids;
+        for (int i : {0, 1, nd, nd + 1})
+            if (std::find(ids.begin(), ids.end(), i) == ids.end()) ids.push_back(i);
+        auto in_ids = [&](int i) { return std::find(ids.begin(), ids.end(), i) != ids.end(); };
+        bool identity = true;
+        for (const auto &kv : E) {
+            const int i = kv.first.first, j = kv.first.second;
+            const double dev = std::fabs(kv.second - (i == j ? 1.0 : 0.0));
+            if (dev == 0.0) continue;
+            identity = false;
+            if (!in_ids(i) || !in_ids(j))
+                return set_error(ICC_BAD_ARG, "tensor-core path: the B-spline extraction is not confined to the two "
+                                              "first and two last control points");
+            // every element whose control points include j also includes i
+            for (int e = std::max(0, j - 2); e <= std::min(nd - 1, j); ++e)
+                if (i < e || i > e + 2)
+                    return set_error(ICC_BAD_ARG, "tensor-core path: the B-spline extraction couples control points "
+                                                  "of different elements");
+        }
+        if (identity) continue;
+        edge.nb[d] = int(ids.size());
+        for (size_t a = 0; a < ids.size(); ++a) {
+            edge.id[d][a] = ids[a];
+            for (size_t b = 0; b < ids.size(); ++b) {
+                auto it = E.find({ids[a], ids[b]});
+                edge.e[d][a][b] = float(it == E.end() ? 0.0 : it->second);
             }
         }
     }
-    return mt;
+    return ICC_OK;
 }
 
 static int mixed_init(Op &op) {
@@ -852,13 +961,14 @@ static int mixed_init(Op &op) {
     if (op.g.nsc >= (1LL << 31)) return set_error(ICC_BAD_ARG, "tensor-core path: more than 2^31 control points");
     if (!op.mixed) op.mixed = new MixedState();
     MixedState &ms = *op.mixed;
-    const int mt = setup_xform(op, ms.xf);
-    if (mt < 0) return ICC_BAD_ARG;
-    // the main element matrix split into TF32 hi/lo in the canonical layout, component c of the
-    // test (row) and trial (column) DOFs at c*32 + [0, 27)
+    std::vector<double> kunif;
+    int rc = setup_edge(op, ms.edge, kunif);
+    if (rc) return rc;
+    // the uniform element matrix split into TF32 hi/lo in the canonical layout, component c of
+    // the test (row) and trial (column) DOFs at c*32 + [0, 27)
     std::vector<float> bm((size_t)2 * kBFl, 0.f);
     {
-        const double *K = op.host_ktypes.data() + (size_t)mt * 81 * 81;
+        const double *K = kunif.data();
         float *hi = bm.data(), *lo = hi + kBFl;
         for (int n = 0; n < 81; ++n)
             for (int k = 0; k < 81; ++k) {
@@ -870,21 +980,25 @@ static int mixed_init(Op &op) {
                 lo[canon(nr, kc, kTcN)] = l;
             }
     }
-    int rc;
     if ((rc = dalloc(&ms.d_bmat, bm.size() / 4, "alloc tc matrices"))) return rc;
     ICC_CUDA(cudaMemcpyAsync(ms.d_bmat, bm.data(), bm.size() * 4, cudaMemcpyHostToDevice, op.stream), "copy tc matrices");
     const Geom &g = op.g;
     {
+        // bit d of a brick: its patch holds boundary control points of direction d
         std::vector<uint8_t> fl((size_t)g.nbricks, 0);
-        const int n[3] = {g.nx, g.ny, g.nz}, be[3] = {kBX, kBY, kBZ};
+        const int be[3] = {kBX, kBY, kBZ}, cp[3] = {g.cx, g.cy, g.cz};
         for (int b = 0; b < g.nbricks; ++b) {
             const int bi[3] = {b % g.nbx, (b / g.nbx) % g.nby, b / (g.nbx * g.nby)};
-            for (int d = 0; d < 3; ++d)
-                for (int e = bi[d] * be[d]; e < std::min(n[d], (bi[d] + 1) * be[d]); ++e)
-                    if ((ms.xf.nonid[d] >> pos_class(e, n[d])) & 1u) fl[(size_t)b] |= uint8_t(1u << d);
+            for (int d = 0; d < 3; ++d) {
+                const int o = bi[d] * be[d], ext = std::min(be[d] + 2, cp[d] - o);
+                for (int a = 0; a < ms.edge.nb[d]; ++a)
+                    if (ms.edge.id[d][a] >= o && ms.edge.id[d][a] < o + ext) fl[(size_t)b] |= uint8_t(1u << d);
+            }
         }
         if ((rc = dalloc(&ms.d_bflags, fl.size(), "alloc brick flags"))) return rc;
+        if ((rc = dalloc(&ms.d_edge, 1, "alloc edge"))) return rc;
         ICC_CUDA(cudaMemcpyAsync(ms.d_bflags, fl.data(), fl.size(), cudaMemcpyHostToDevice, op.stream), "copy brick flags");
+        ICC_CUDA(cudaMemcpyAsync(ms.d_edge, &ms.edge, sizeof(Edge), cudaMemcpyHostToDevice, op.stream), "copy edge");
         ICC_CUDA(cudaStreamSynchronize(op.stream), "copy brick flags");
     }
     const size_t n = (size_t)op.ndof;
@@ -905,7 +1019,7 @@ static int mixed_init(Op &op) {
         // the fused steps of concurrent solves (icc_pcg_solve_batched) can share the GPU
         const long long need = (op.g.nsc + kTailThreads - 1) / kTailThreads;
         ms.tail_grid = (int)std::max(1LL, std::min<long long>((long long)std::max(1, std::min(per_sm, 4)) * op.num_sms, need));
-        if ((rc = dalloc(&ms.d_tail_part, (size_t)3 * ms.tail_grid, "alloc mixed"))) return rc;
+        if ((rc = dalloc(&ms.d_tail_part, (size_t)7 * ms.tail_grid, "alloc mixed"))) return rc;
         if ((rc = dalloc(&ms.d_grid_ctr, 1, "alloc mixed"))) return rc;
         ICC_CUDA(cudaMemsetAsync(ms.d_grid_ctr, 0, sizeof(unsigned long long), op.stream), "clear grid counter");
     }
@@ -926,7 +1040,7 @@ void mixed_release(Op &op) {
     if (!op.mixed) return;
     MixedState &ms = *op.mixed;
     if (ms.graph) cudaGraphExecDestroy(ms.graph);
-    void *bufs[] = {ms.d_bmat, ms.d_bflags, ms.d_scale32, ms.d_patch32, ms.d_rhs32, ms.d_x32, ms.d_r32, ms.d_p32,
+    void *bufs[] = {ms.d_bmat, ms.d_bflags, ms.d_edge, ms.d_scale32, ms.d_patch32, ms.d_rhs32, ms.d_x32, ms.d_r32, ms.d_p32,
                     ms.d_ap32, ms.d_inv32, ms.d_xm32, ms.d_x64, ms.d_r64, ms.d_y64, ms.d_scalars,
                     ms.d_err, ms.d_state, ms.d_tail_part, ms.d_grid_ctr};
     for (void *p : bufs)
@@ -956,7 +1070,7 @@ __global__ void mask_copy_kernel(long long n, const float *__restrict__ x, const
 static void launch_apply_tc(Op &op, const float *xin, const PcgState *st) {
     MixedState &ms = *op.mixed;
     const int grid = std::min(op.num_sms, op.g.nbricks);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, ms.d_bmat, ms.xf,
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, ms.d_bmat, ms.d_edge,
                                                               ms.d_bflags, ms.d_patch32, ms.d_err, st);
 }
 
@@ -970,8 +1084,9 @@ static void enqueue_apply_tc(Op &op, const float *x, float *y) {
         xin = ms.d_xm32;
     }
     launch_apply_tc(op, xin, nullptr);
-    gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, x, op.d_mask, op.mask_mode,
-                                                                       y, nullptr, nullptr);
+    gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, ms.d_edge, x, op.d_mask,
+                                                                       op.mask_mode,
+                                                                       op.extra32(), y, nullptr, nullptr);
 }
 
 // One iteration of the FP32 PCG: the tensor-core apply and the fused vector step.  With
@@ -991,8 +1106,8 @@ static cudaError_t enqueue_inner_iteration(Op &op) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pcg_tail_kernel, op.g, (const float *)ms.d_patch32,
-                              (const uint8_t *)(zero || ident ? op.d_mask : nullptr), op.mask_mode,
+    return cudaLaunchKernelEx(&cfg, pcg_tail_kernel, op.g, (const float *)ms.d_patch32, (const Edge *)ms.d_edge,
+                              (const uint8_t *)(zero || ident ? op.d_mask : nullptr), op.mask_mode, op.extra32(),
                               (const float *)ms.d_inv32, ms.d_x32, ms.d_r32, ms.d_p32, ident ? ms.d_xm32 : nullptr,
                               ms.d_ap32, ms.d_tail_part, ms.d_state, ms.d_grid_ctr, ms.d_err,
                               ms.grid_wait_limit);
@@ -1026,6 +1141,14 @@ int mixed_apply_f32(Op &op, const float *x, float *y) {
     return ICC_OK;
 }
 
+// The captured iteration graph holds kernel arguments by value; it is rebuilt after they change.
+void mixed_invalidate_graph(Op &op) {
+    if (!op.mixed || !op.mixed->graph) return;
+    cudaGraphExecDestroy(op.mixed->graph);
+    op.mixed->graph = nullptr;
+    op.mixed->graph_batch = 0;
+}
+
 // Polls of a grid barrier before the fused vector step gives up (ICC_TIMEOUT).
 int mixed_set_wait_limit(Op &op, long long polls) {
     int rc = mixed_init(op);
@@ -1046,8 +1169,9 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
         cudaEventRecord(ev[3 * r], op.stream);
         launch_apply_tc(op, x, nullptr);
         cudaEventRecord(ev[3 * r + 1], op.stream);
-        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, x, op.d_mask,
-                                                                           ICC_MASK_NONE, y, nullptr, nullptr);
+        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, ms.d_edge, x, op.d_mask,
+                                                                           ICC_MASK_NONE, op.extra32(), y, nullptr,
+                                                                           nullptr);
         cudaEventRecord(ev[3 * r + 2], op.stream);
     }
     cudaError_t e = cudaEventSynchronize(ev.back());
@@ -1111,6 +1235,8 @@ ru_replace_finalize(const double *__restrict__ partials, int np, PcgState *st) {
     if (threadIdx.x == 0) {
         st->beta = rz / st->rz_prev;
         st->rz_old = rz;
+        st->rr_old = rr;
+        st->fresh = 1;   // the next fused step takes r'r and r'z from here
         st->rel_res = sqrt(rr) / st->norm_b;
         st->status = 0;
     }

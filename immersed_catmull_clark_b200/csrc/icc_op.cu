@@ -162,10 +162,12 @@ apply_f64_kernel(Geom g, const double *__restrict__ x, const uint8_t *__restrict
 }
 
 // Jacobi diagonal sum_e s_e K_type(e)[a,a]; elements visited in increasing index so the sum
-// rounds exactly as the assembled CSR entry (rust/src/sparse.rs:166-172, then :70-78).
+// rounds exactly as the assembled CSR entry (rust/src/sparse.rs:166-172, then :70-78).  With a
+// sparse term, its diagonal is added last, as the reference adds the stabilisation's diagonal to
+// the stiffness diagonal (rust/src/topopt_immersed.rs:165-167).
 __global__ void __launch_bounds__(kVecThreads)
 diagonal_kernel(Geom g, const double *__restrict__ scale, const int *__restrict__ type_id,
-                const double *__restrict__ kdiag, double *__restrict__ d) {
+                const double *__restrict__ kdiag, const double *__restrict__ extra, double *__restrict__ d) {
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < g.nsc;
          n += (long long)gridDim.x * blockDim.x) {
         int ix = int(n % g.cx), iy = int((n / g.cx) % g.cy), iz = int(n / ((long long)g.cx * g.cy));
@@ -181,6 +183,11 @@ diagonal_kernel(Geom g, const double *__restrict__ scale, const int *__restrict_
                     s1 = __dadd_rn(s1, __dmul_rn(s, kd[27 + a]));
                     s2 = __dadd_rn(s2, __dmul_rn(s, kd[54 + a]));
                 }
+        if (extra) {
+            s0 += extra[n];
+            s1 += extra[g.nsc + n];
+            s2 += extra[2 * g.nsc + n];
+        }
         d[n] = s0;
         d[g.nsc + n] = s1;
         d[2 * g.nsc + n] = s2;
@@ -208,6 +215,8 @@ pcg_init_finalize(const double *__restrict__ partials, int np, PcgState *st, dou
         st->status = max_iter > 0 ? 0 : kStatMaxIter;
         st->alpha = st->beta = st->p_ap = 0.0;
         st->rz_prev = rz;
+        st->rr_old = bb;
+        st->fresh = 1;
         st->repl_res = 1.0;
         st->repl_delta = 0.0;
         st->repl_iter = 0;
@@ -231,7 +240,8 @@ static int dev_alloc(T **p, size_t count, const char *what) {
 Op::~Op() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     void *bufs[] = {d_x_in, d_y_out, d_scale, d_kfrag, d_kdiag, d_type_id, d_tile_start, d_tile_type, d_tile_elem,
-                    d_mask, d_patch, d_x, d_r, d_p, d_ap, d_inv, d_b, d_diag, d_partials, d_state, d_counter};
+                    d_mask, d_patch, d_x, d_r, d_p, d_ap, d_inv, d_b, d_diag, d_partials, d_state, d_counter,
+                    d_sp_ptr, d_sp_idx, d_sp_val, d_sp_val32, d_sp_diag};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h_state) cudaFreeHost(h_state);
@@ -378,7 +388,15 @@ int Op::set_scale_dev(const double *scale_dev) {
 
 int Op::set_mask(const uint8_t *free_mask, int mode) {
     if (mode < 0 || mode > 2) return set_error(ICC_BAD_ARG, "mask_mode must be 0, 1 or 2");
-    mask_mode = (mode != ICC_MASK_NONE && free_mask) ? mode : ICC_MASK_NONE;
+    const int new_mode = (mode != ICC_MASK_NONE && free_mask) ? mode : ICC_MASK_NONE;
+    if (new_mode != mask_mode) {
+        // the iteration graphs hold the mask mode by value: rebuild them on the next solve
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        graph_batch = 0;
+        mixed_invalidate_graph(*this);
+    }
+    mask_mode = new_mode;
     std::vector<uint8_t> ones;
     const uint8_t *src = free_mask;
     if (!src) {
@@ -390,12 +408,80 @@ int Op::set_mask(const uint8_t *free_mask, int mode) {
     return ICC_OK;
 }
 
+// The extra sparse term from triplets (duplicates summed in input order, columns sorted per row).
+// Replaces any previous term; count = 0 removes it.
+int Op::set_extra(int64_t count, const int64_t *rows, const int64_t *cols, const double *vals) {
+    for (int64_t k = 0; k < count; ++k)
+        if (rows[k] < 0 || rows[k] >= ndof || cols[k] < 0 || cols[k] >= ndof)
+            return set_error(ICC_BAD_ARG, "icc_op_set_extra_triplets: index out of range");
+    if (count >= (1LL << 31) || ndof >= (1LL << 31))
+        return set_error(ICC_BAD_ARG, "icc_op_set_extra_triplets: more than 2^31 entries or DOFs");
+    // counting sort by row, then a stable sort by column inside each row, then merge
+    std::vector<int> ptr((size_t)ndof + 1, 0);
+    for (int64_t k = 0; k < count; ++k) ptr[(size_t)rows[k] + 1]++;
+    for (int64_t i = 0; i < ndof; ++i) ptr[(size_t)i + 1] += ptr[(size_t)i];
+    std::vector<int64_t> order((size_t)count);
+    {
+        std::vector<int> next(ptr.begin(), ptr.end() - 1);
+        for (int64_t k = 0; k < count; ++k) order[(size_t)next[(size_t)rows[k]]++] = k;
+    }
+    std::vector<int> mptr((size_t)ndof + 1, 0), midx;
+    std::vector<double> mval, diag((size_t)ndof, 0.0);
+    midx.reserve((size_t)count);
+    mval.reserve((size_t)count);
+    for (int64_t i = 0; i < ndof; ++i) {
+        auto b = order.begin() + ptr[(size_t)i], e = order.begin() + ptr[(size_t)i + 1];
+        std::stable_sort(b, e, [&](int64_t a, int64_t c) { return cols[a] < cols[c]; });
+        for (auto it = b; it != e; ++it) {
+            if (it != b && cols[*it] == cols[*(it - 1)]) mval.back() += vals[*it];
+            else {
+                midx.push_back(int(cols[*it]));
+                mval.push_back(vals[*it]);
+            }
+        }
+        mptr[(size_t)i + 1] = int(midx.size());
+        for (int k = mptr[(size_t)i]; k < mptr[(size_t)i + 1]; ++k)
+            if (midx[(size_t)k] == i) diag[(size_t)i] = mval[(size_t)k];
+    }
+    void *old[] = {d_sp_ptr, d_sp_idx, d_sp_val, d_sp_val32, d_sp_diag};
+    ICC_CUDA(cudaStreamSynchronize(stream), "extra term: drain");
+    for (void *p : old)
+        if (p) cudaFree(p);
+    d_sp_ptr = d_sp_idx = nullptr;
+    d_sp_val = d_sp_diag = nullptr;
+    d_sp_val32 = nullptr;
+    sp_nnz = 0;
+    if (midx.empty()) return ICC_OK;
+    const size_t nnz = midx.size();
+    std::vector<float> v32(nnz);
+    for (size_t k = 0; k < nnz; ++k) v32[k] = float(mval[k]);
+    int rc;
+    if ((rc = dev_alloc(&d_sp_ptr, mptr.size(), "alloc extra term")) || (rc = dev_alloc(&d_sp_idx, nnz, "alloc extra term")) ||
+        (rc = dev_alloc(&d_sp_val, nnz, "alloc extra term")) || (rc = dev_alloc(&d_sp_val32, nnz, "alloc extra term")) ||
+        (rc = dev_alloc(&d_sp_diag, (size_t)ndof, "alloc extra term")))
+        return rc;
+    ICC_CUDA(cudaMemcpyAsync(d_sp_ptr, mptr.data(), mptr.size() * 4, cudaMemcpyHostToDevice, stream), "copy extra term");
+    ICC_CUDA(cudaMemcpyAsync(d_sp_idx, midx.data(), nnz * 4, cudaMemcpyHostToDevice, stream), "copy extra term");
+    ICC_CUDA(cudaMemcpyAsync(d_sp_val, mval.data(), nnz * 8, cudaMemcpyHostToDevice, stream), "copy extra term");
+    ICC_CUDA(cudaMemcpyAsync(d_sp_val32, v32.data(), nnz * 4, cudaMemcpyHostToDevice, stream), "copy extra term");
+    ICC_CUDA(cudaMemcpyAsync(d_sp_diag, diag.data(), diag.size() * 8, cudaMemcpyHostToDevice, stream), "copy extra term");
+    ICC_CUDA(cudaStreamSynchronize(stream), "copy extra term");
+    sp_nnz = (int64_t)nnz;
+    // graphs captured with the previous term's pointers are rebuilt on the next solve
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    graph_batch = 0;
+    mixed_invalidate_graph(*this);
+    return ICC_OK;
+}
+
 // Enqueue y = A x on the op's stream (FP64).  partials != null also forms p'y per CTA.
 void Op::enqueue_apply(const double *x, double *y, double *partials, const PcgState *st) {
     apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
         g, x, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
         st);
-    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, x, d_mask, mask_mode, y, partials, st);
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, nullptr, x, d_mask, mask_mode, extra64(), y,
+                                                                  partials, st);
 }
 
 int Op::apply_dev(const double *x, double *y) {
@@ -405,7 +491,8 @@ int Op::apply_dev(const double *x, double *y) {
 }
 
 int Op::diagonal_dev(double *d) {
-    diagonal_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(g, d_scale, d_type_id, d_kdiag, d);
+    diagonal_kernel<<<vec_blocks, kVecThreads, 0, stream>>>(g, d_scale, d_type_id, d_kdiag, sp_nnz ? d_sp_diag : nullptr,
+                                                            d);
     ICC_CUDA(cudaGetLastError(), "diagonal launch");
     return ICC_OK;
 }
@@ -432,7 +519,8 @@ void Op::enqueue_pcg_iteration() {
     apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
         g, d_p, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
         d_state);
-    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, d_p, d_mask, mask_mode, d_ap, d_partials,
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, nullptr, d_p, d_mask, mask_mode, extra64(), d_ap,
+                                                                  d_partials,
                                                                   d_state, d_state, d_counter);
     pcg_update_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials,
                                                                       d_state, d_state, d_counter);
@@ -540,6 +628,14 @@ int icc_op_update_scale(icc_op *op, const double *scale) {
     if (!op) return set_error(ICC_BAD_ARG, "icc_op_update_scale: null op");
     cudaSetDevice(op->op.device);
     return op->op.set_scale(scale);
+}
+
+int icc_op_set_extra_triplets(icc_op *op, int64_t count, const int64_t *rows, const int64_t *cols,
+                              const double *vals) {
+    if (!op || count < 0 || (count > 0 && (!rows || !cols || !vals)))
+        return set_error(ICC_BAD_ARG, "icc_op_set_extra_triplets: bad argument");
+    cudaSetDevice(op->op.device);
+    return op->op.set_extra(count, rows, cols, vals);
 }
 
 int icc_op_update_mask(icc_op *op, const uint8_t *free_mask, int32_t mask_mode) {
@@ -715,8 +811,8 @@ int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t
             o.g, x_dev, o.d_mask, o.mask_mode != ICC_MASK_NONE, o.d_scale, o.d_kfrag, o.d_tile_start, o.d_tile_type,
             o.d_tile_elem, o.d_patch, nullptr);
         cudaEventRecord(ev[3 * r + 1], o.stream);
-        icc::gather_kernel<double><<<o.vec_blocks, icc::kVecThreads, 0, o.stream>>>(o.g, o.d_patch, x_dev, o.d_mask,
-                                                                                o.mask_mode, y_dev, nullptr, nullptr);
+        icc::gather_kernel<double><<<o.vec_blocks, icc::kVecThreads, 0, o.stream>>>(
+            o.g, o.d_patch, nullptr, x_dev, o.d_mask, o.mask_mode, o.extra64(), y_dev, nullptr, nullptr);
         cudaEventRecord(ev[3 * r + 2], o.stream);
     }
     cudaError_t e = cudaEventSynchronize(ev.back());

@@ -106,6 +106,16 @@ void icc_op_destroy(icc_op *op);
  * (rust/src/sparse.rs:160, called from rust/src/topopt_iga.rs:131-134). */
 int icc_op_update_scale(icc_op *op, const double *scale);
 int icc_op_update_mask(icc_op *op, const uint8_t *free_mask, int32_t mask_mode);
+/* A sparse term S added to the operator: y = mask rule of (K + S)(m .* x), i.e. the closures that
+ * add a stabilisation matrix to the stiffness inside PcgSolver::solve (rust/src/topopt_immersed.rs:
+ * 174-183 k.matvec + stab.matvec; rust/src/immersed.rs:514-548 + :558-566, the stabilisation
+ * assembled into the stiffness).  Triplets (row, col, value) over the DOF numbering, duplicates
+ * summed (CsrMatrix::from_triplets, rust/src/sparse.rs:16-58); count = 0 removes the term.  The
+ * diagonal (icc_op_diagonal, and the solve's default preconditioner) includes S's diagonal; the
+ * FP64 forms apply S in FP64, the tensor-core FP32 form in FP32.  Element energies stay those of
+ * K alone (as the reference computes them from the element matrices). */
+int icc_op_set_extra_triplets(icc_op *op, int64_t count, const int64_t *rows, const int64_t *cols,
+                              const double *vals);
 /* y = A x with A the masked operator (host arrays of length n = ndof); mirrors the closure
  * around CsrMatrix::matvec (rust/src/sparse.rs:60-68). */
 int icc_op_apply(icc_op *op, const double *x, double *y, int64_t n);
@@ -209,6 +219,19 @@ int icc_topopt_run(icc_topopt *t, int32_t max_iter, double *compliance, double *
  * sub[0] x sub[1] x sub[2] cell midpoints inside.  Computed on the device; host arrays of
  * res[0] res[1] res[2] cells. */
 int icc_cylinder_weights(const int64_t res[3], const int32_t sub[3], double radius, double *weights, int8_t *status);
+
+/* ---- cut-cell stabilisation (triplets for icc_op_set_extra_triplets) ---------------------------
+ * status[nel] per cell: 1 inside, 0 outside, -1 cut.  Both return *count triplets; called with
+ * rows = cols = vals = NULL they only report the count, else they fill up to capacity entries.
+ * rust/src/immersed.rs:224-370 ghost_penalty: gamma E h^(2p-1) sum_F int_F [d_n^p u].[d_n^p v] over
+ * interior faces between two active cells of which at least one is cut, per component. */
+int icc_ghost_penalty(const icc_space *sp, const int8_t *status, double gamma, double young, int64_t *rows,
+                      int64_t *cols, double *vals, int64_t capacity, int64_t *count);
+/* rust/src/immersed.rs:156-222 legacy_stabilization (the MATLAB heuristic kept for the reference's
+ * fixture): zero-sum diagonal blocks on shared control points and springs of stiffness
+ * gamma mean(h) between the faces' non-shared control points. */
+int icc_legacy_stabilization(const icc_space *sp, const int8_t *status, double gamma, int64_t *rows, int64_t *cols,
+                             double *vals, int64_t capacity, int64_t *count);
 
 /* ---- diagnostics (no reference counterpart) -------------------------------------------------
  * Times `reps` FP64 applies of x_dev on the handle's stream with CUDA events around each of the

@@ -1247,6 +1247,170 @@ void orc_cylinders_weights(const int *res, const int *sub, double radius, double
     free(inside);
 }
 
+/* rust/src/iga/basis.rs:72-135 basis_funs_ders (The NURBS Book A2.3): the p+1 nonzero basis
+ * functions at x on knot span s and their derivatives up to order n (n <= p <= 4):
+ * ders[k * (p + 1) + r] = d^k/dx^k N_{s - p + r}(x). */
+static void ders_basis_funs(const double *knots, int p, double x, int n, int s, double *ders) {
+    double ndu[5][5], left[5], right[5], a[2][5];
+    ndu[0][0] = 1.0;
+    for (int j = 1; j <= p; j++) {
+        left[j] = x - knots[s + 1 - j];
+        right[j] = knots[s + j] - x;
+        double saved = 0.0;
+        for (int r = 0; r < j; r++) {
+            ndu[j][r] = right[r + 1] + left[j - r];
+            double temp = ndu[r][j - 1] / ndu[j][r];
+            ndu[r][j] = saved + right[r + 1] * temp;
+            saved = left[j - r] * temp;
+        }
+        ndu[j][j] = saved;
+    }
+    for (int k = 0; k <= n; k++)
+        for (int j = 0; j <= p; j++) ders[k * (p + 1) + j] = 0.0;
+    for (int j = 0; j <= p; j++) ders[j] = ndu[j][p];
+    for (int r = 0; r <= p; r++) {
+        int s1 = 0, s2 = 1;
+        a[0][0] = 1.0;
+        int kmax = n < p ? n : p;
+        for (int k = 1; k <= kmax; k++) {
+            double d = 0.0;
+            int rk = r - k, pk = p - k;
+            if (r >= k) {
+                a[s2][0] = a[s1][0] / ndu[pk + 1][rk];
+                d = a[s2][0] * ndu[rk][pk];
+            }
+            int j1 = rk >= -1 ? 1 : -rk;
+            int j2 = (r - 1) <= pk ? k - 1 : p - r;
+            for (int j = j1; j <= j2; j++) {
+                a[s2][j] = (a[s1][j] - a[s1][j - 1]) / ndu[pk + 1][rk + j];
+                d += a[s2][j] * ndu[rk + j][pk];
+            }
+            if (r <= pk) {
+                a[s2][k] = -a[s1][k - 1] / ndu[pk + 1][r];
+                d += a[s2][k] * ndu[r][pk];
+            }
+            ders[k * (p + 1) + r] = d;
+            int t = s1; s1 = s2; s2 = t;
+        }
+    }
+    double fac = (double)p;
+    int kmax = n < p ? n : p;
+    for (int k = 1; k <= kmax; k++) {
+        for (int j = 0; j <= p; j++) ders[k * (p + 1) + j] *= fac;
+        fac *= (double)(p - k);
+    }
+}
+
+/* rust/src/immersed.rs:224-370 ghost_penalty: returns the triplet count and fills rows/cols/vals
+ * when they are non-NULL (call once with NULL to size the buffers). */
+i64 orc_ghost_penalty(const orc_space *sp, const int8_t *status, double gamma, double young, i64 *ri, i64 *ci,
+                      double *vi) {
+    int dim = sp->dim;
+    double h[ORC_MAXD];
+    for (int d = 0; d < dim; d++) h[d] = sp->lengths[d] / (double)sp->nel_dir[d];
+    double hsum = 0.0;
+    for (int d = 0; d < dim; d++) hsum += h[d];
+    double h_char = hsum / (double)dim;
+    /* 1-D tangential mass matrices per direction and element (physical) */
+    double *mass[ORC_MAXD];
+    for (int d = 0; d < dim; d++) {
+        const orc_space1d *u = &sp->univ[d];
+        int nl = u->degree + 1;
+        mass[d] = (double *)calloc((size_t)u->nel * nl * nl, sizeof(double));
+        for (int e = 0; e < u->nel; e++) {
+            double *m = mass[d] + (size_t)e * nl * nl;
+            for (int q = 0; q < u->nquad; q++) {
+                double w = u->qw[e * u->nquad + q] * sp->lengths[d];
+                const double *sh = u->shape + (size_t)(e * u->nquad + q) * nl;
+                for (int a = 0; a < nl; a++)
+                    for (int b = 0; b < nl; b++) m[a * nl + b] += w * sh[a] * sh[b];
+            }
+        }
+    }
+    /* 1-D jumps of the p-th derivative across interior break k: indices lo..hi and values */
+    int *jlo[ORC_MAXD], *jn[ORC_MAXD];
+    double *jval[ORC_MAXD];
+    for (int d = 0; d < dim; d++) {
+        const orc_space1d *u = &sp->univ[d];
+        int p = u->degree, nl = p + 1;
+        double lp = pow(sp->lengths[d], (double)p);
+        jlo[d] = (int *)calloc((size_t)u->nel, sizeof(int));
+        jn[d] = (int *)calloc((size_t)u->nel, sizeof(int));
+        jval[d] = (double *)calloc((size_t)u->nel * 2 * nl, sizeof(double));
+        for (int k = 1; k < u->nel; k++) {
+            double x = u->breaks[k];
+            int lf = u->connectivity[(k - 1) * nl], rf = u->connectivity[k * nl];
+            double dl[25], dr[25];
+            ders_basis_funs(u->knots, p, x, p, lf + p, dl);
+            ders_basis_funs(u->knots, p, x, p, rf + p, dr);
+            int lo = lf < rf ? lf : rf;
+            int hi = (lf + p) > (rf + p) ? (lf + p) : (rf + p);
+            jlo[d][k] = lo;
+            jn[d][k] = hi - lo + 1;
+            for (int g = lo; g <= hi; g++) {
+                double r_val = (g >= rf && g <= rf + p) ? dr[p * nl + (g - rf)] : 0.0;
+                double l_val = (g >= lf && g <= lf + p) ? dl[p * nl + (g - lf)] : 0.0;
+                jval[d][(size_t)k * 2 * nl + (g - lo)] = (r_val - l_val) / lp;
+            }
+        }
+    }
+    i64 nt = 0;
+    for (int d = 0; d < dim; d++) {
+        int p = sp->degree[d];
+        double coef = gamma * young * pow(h_char, (double)(2 * p - 1));
+        for (i64 e2 = 0; e2 < sp->nel; e2++) {
+            int s2[ORC_MAXD], s1[ORC_MAXD];
+            unravel(e2, sp->nel_dir, dim, s2);
+            if (s2[d] == 0) continue;
+            for (int dd = 0; dd < dim; dd++) s1[dd] = s2[dd];
+            s1[d] -= 1;
+            i64 lin1 = 0, stride = 1;
+            for (int dd = 0; dd < dim; dd++) { lin1 += (i64)s1[dd] * stride; stride *= sp->nel_dir[dd]; }
+            int a1 = status[lin1] == 1 || status[lin1] == -1, a2 = status[e2] == 1 || status[e2] == -1;
+            if (!(a1 && a2 && (status[lin1] == -1 || status[e2] == -1))) continue;
+            int nl_d = sp->univ[d].degree + 1;
+            const double *jv = jval[d] + (size_t)s2[d] * 2 * nl_d;
+            int sizes[ORC_MAXD], first[ORC_MAXD];
+            for (int dd = 0; dd < dim; dd++) {
+                if (dd == d) { sizes[dd] = jn[d][s2[d]]; first[dd] = jlo[d][s2[d]]; }
+                else {
+                    const orc_space1d *u = &sp->univ[dd];
+                    sizes[dd] = u->degree + 1;
+                    first[dd] = u->connectivity[s2[dd] * (u->degree + 1)];
+                }
+            }
+            int nloc = 1;
+            for (int dd = 0; dd < dim; dd++) nloc *= sizes[dd];
+            i64 *gidx = (i64 *)malloc(sizeof(i64) * (size_t)nloc);
+            int (*sa)[ORC_MAXD] = malloc(sizeof(int) * ORC_MAXD * (size_t)nloc);
+            for (int a = 0; a < nloc; a++) {
+                unravel(a, sizes, dim, sa[a]);
+                i64 g = 0, st = 1;
+                for (int dd = 0; dd < dim; dd++) { g += (i64)(first[dd] + sa[a][dd]) * st; st *= sp->ndof_dir[dd]; }
+                gidx[a] = g;
+            }
+            for (int a = 0; a < nloc; a++)
+                for (int b = 0; b < nloc; b++) {
+                    double v = coef * jv[sa[a][d]] * jv[sa[b][d]];
+                    for (int t = 0; t < dim; t++) {
+                        if (t == d) continue;
+                        int nl = sp->nsh_dir[t];
+                        v *= mass[t][((size_t)s2[t] * nl + sa[a][t]) * nl + sa[b][t]];
+                    }
+                    if (v == 0.0) continue;
+                    for (int c = 0; c < dim; c++) {
+                        if (ri) { ri[nt] = c * sp->ndof_sc + gidx[a]; ci[nt] = c * sp->ndof_sc + gidx[b]; vi[nt] = v; }
+                        nt++;
+                    }
+                }
+            free(gidx);
+            free(sa);
+        }
+    }
+    for (int d = 0; d < dim; d++) { free(mass[d]); free(jlo[d]); free(jn[d]); free(jval[d]); }
+    return nt;
+}
+
 /* rust/src/immersed.rs:168-222 legacy_stabilization; returns the triplet count and fills
  * rows/cols/vals when they are non-NULL (call once with NULL to size the buffers). */
 i64 orc_legacy_stabilization(const orc_space *sp, const int8_t *status, double gamma, i64 *ri, i64 *ci,

@@ -82,6 +82,8 @@ def lib():
         L.orc_cylinders_weights.argtypes = [i32p, i32p, C.c_double, f64p, i8p]
         L.orc_legacy_stabilization.argtypes = [vp, i8p, C.c_double, vp, vp, vp]
         L.orc_legacy_stabilization.restype = C.c_int64
+        L.orc_ghost_penalty.argtypes = [vp, i8p, C.c_double, C.c_double, vp, vp, vp]
+        L.orc_ghost_penalty.restype = C.c_int64
         L.orc_immersed_bc.argtypes = [vp, u8p, f64p]
         L.orc_solve_immersed.argtypes = [vp, u8p, f64p, C.c_double, C.c_int64, f64p,
                                          C.POINTER(C.c_int64), C.POINTER(C.c_double),
@@ -318,6 +320,15 @@ def legacy_stabilization(sp, status, gamma):
     n = lib().orc_legacy_stabilization(sp._h, st, gamma, None, None, None)
     r = np.zeros(n, dtype=np.int64); c = np.zeros(n, dtype=np.int64); v = np.zeros(n)
     lib().orc_legacy_stabilization(sp._h, st, gamma, _ptr(r), _ptr(c), _ptr(v))
+    return r, c, v
+
+
+def ghost_penalty(sp, status, gamma, young):
+    """rust/src/immersed.rs:224-370 ghost_penalty as triplets (rows, cols, vals)."""
+    st = np.ascontiguousarray(status, dtype=np.int8)
+    n = lib().orc_ghost_penalty(sp._h, st, gamma, young, None, None, None)
+    r = np.zeros(n, dtype=np.int64); c = np.zeros(n, dtype=np.int64); v = np.zeros(n)
+    lib().orc_ghost_penalty(sp._h, st, gamma, young, _ptr(r), _ptr(c), _ptr(v))
     return r, c, v
 
 
