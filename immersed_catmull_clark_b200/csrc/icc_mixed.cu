@@ -113,9 +113,14 @@ constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][
 constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * 3 * kPVol + 2 * kZFl) * 4;  // 202,272 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
+// Each test may sleep up to kWaitSleepNs; with kWaitLimit tests a wait gives up after at most
+// ~4 s, and after at least kWaitLimit quick tests (~0.1 s) if the hardware ignores the hint --
+// both far beyond any wait of a working kernel (a brick takes a few microseconds).
+constexpr uint32_t kWaitSleepNs = 1000;
+
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
     for (long long i = 0; i < kWaitLimit; ++i) {
-        if (tc::mbar_try_wait(bar, parity)) return true;
+        if (tc::mbar_try_wait_sleep(bar, parity, kWaitSleepNs)) return true;
         if (*abort_flag) return false;
     }
     *abort_flag = 1;
