@@ -138,6 +138,8 @@ struct Op {
     int set_mask(const uint8_t *free_mask, int mode);
     int set_extra(int64_t count, const int64_t *rows, const int64_t *cols, const double *vals);
     void enqueue_apply(const double *x, double *y, double *partials, const PcgState *st);
+    void enqueue_apply_on(cudaStream_t s, const double *x, double *y);   // y = A x on stream s
+    void enqueue_diagonal(double *d, cudaStream_t s);                     // the diagonal on stream s
     int apply_dev(const double *x, double *y);
     int diagonal_dev(double *d);
     int ensure_pcg_buffers();
@@ -155,6 +157,14 @@ int mixed_on_scale_update(Op &op);
 int mixed_apply_f32(Op &op, const float *x, float *y);
 int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms);
 int mixed_set_wait_limit(Op &op, long long polls);
+struct VecSet;   // the vectors of one system of a mixed solve (icc_mixed.cu)
+int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const std::vector<VecSet *> &vsets,
+                      const double *const *b, const double *const *diag, const double *tol, const int64_t *max_iter,
+                      const icc_solve_opts &opts, double *const *x, int *status, int64_t *iters, double *rel_res,
+                      int64_t *replacements);
+VecSet *mixed_vecset_create(Op &op);
+void mixed_vecset_destroy(VecSet *v);
+VecSet *mixed_own_vecset(Op &op);
 void mixed_invalidate_graph(Op &op);
 int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter,
                 const icc_solve_opts &opts, double *x, int64_t *iters, double *rel_res);

@@ -54,25 +54,55 @@ __host__ __device__ __forceinline__ int canon(int row, int k, int rows) {
     return (k >> 2) * (rows / 8) * 32 + (row >> 3) * 32 + (row & 7) * 4 + (k & 3);
 }
 
+// One system of a mixed solve as the kernels see it: the operator data of its handle and its own
+// FP32 vectors.  A solve of one system is a batch of one; a batch of several (designs of uneven
+// sizes, or load cases of one operator) runs every iteration as one persistent apply over all
+// bricks of all systems and one fused vector step whose CTAs are shared out among the systems.
+struct TcInst {
+    Geom g;
+    int brick0;                  // first brick of the system in the batch's brick numbering
+    int cta0, ncta;              // CTAs of the fused vector step that serve it
+    float kfac;                  // the system's K_u = kfac * the batch's K_u (same element shape)
+    const float *xin;            // input of the brick apply (p, or the masked copy pm)
+    const float *scale;          // s_e (FP32)
+    const uint8_t *bflags;
+    const Edge *edge;
+    float *patch;                // brick partials [nbricks][3][kPVol]
+    const uint8_t *mask;         // output rule of the fused vector step (null: none)
+    int mask_mode;
+    Sparse<float> sp;
+    const float *inv;
+    float *x, *r, *p, *pm, *ap;
+    double *part;                // [7][ncta] partial sums of the fused vector step
+    PcgState *st;                // null for a plain apply: every brick is active
+};
+
+// The FP32 and FP64 vectors and the PCG state of one system of a mixed solve.
+struct VecSet {
+    float *patch32 = nullptr, *rhs32 = nullptr, *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *ap32 = nullptr,
+          *xm32 = nullptr, *inv32 = nullptr;   // xm32: masked input of the brick apply (ICC_MASK_IDENTITY)
+    double *x64 = nullptr, *r64 = nullptr, *y64 = nullptr;
+    double *part = nullptr;  // [7][tail CTAs]
+    int part_cap = 0;
+};
+
 struct MixedState {
     bool ready = false;
     float4 *d_bmat = nullptr;        // K_u split [hi, lo][kBFl] in the canonical layout
+    std::vector<double> kunif;       // K_u (host), to compare systems of a batch
     Edge edge{};
     Edge *d_edge = nullptr;          // the same in device memory, for the node-side passes
     uint8_t *d_bflags = nullptr;     // per brick: bit d set when its patch holds boundary points of d
     float *d_scale32 = nullptr;
-    float *d_patch32 = nullptr;
-    float *d_rhs32 = nullptr, *d_x32 = nullptr, *d_r32 = nullptr, *d_p32 = nullptr, *d_ap32 = nullptr,
-          *d_inv32 = nullptr, *d_xm32 = nullptr;   // xm32: masked input of the brick apply
-    double *d_x64 = nullptr, *d_r64 = nullptr, *d_y64 = nullptr, *d_scalars = nullptr;
+    double *d_scalars = nullptr, *h_scalars = nullptr;
     int *d_err = nullptr;
-    double *d_tail_part = nullptr;            // [7][tail_grid] partial sums of the fused vector step
-    unsigned long long *d_grid_ctr = nullptr;  // grid barrier counter of the fused vector step
-    int tail_grid = 0;
-    long long grid_wait_limit = kGridWaitLimit;
     int *h_err = nullptr;                      // pinned copy of d_err read after every graph batch
+    unsigned long long *d_grid_ctr = nullptr;  // grid barrier counter of the fused vector step
+    int tail_per_sm = 1;                       // resident CTAs of the fused vector step per SM
+    long long grid_wait_limit = kGridWaitLimit;
+    VecSet v;                                  // the handle's own system
+    TcInst *d_inst = nullptr;                  // its one-entry instance table
     PcgState *d_state = nullptr, *h_state = nullptr;
-    double *h_scalars = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_batch = 0;
     long long graph_limit = 0;   // grid_wait_limit the graph was captured with
@@ -83,18 +113,20 @@ struct MixedState {
 // ------------------------------------------------------------------------------------------
 
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
-// One CTA per SM walks bricks blockIdx.x, blockIdx.x + gridDim.x, ...  Roles (25 warps):
+// One CTA per SM walks the bricks blockIdx.x, blockIdx.x + gridDim.x, ... of the batch's brick
+// numbering (all bricks of all systems), skipping systems whose solve has stopped.  Roles
+// (25 warps):
 //   warps 0-11 (builders, warp 4 c + q: component c of z-layer q): fetch the input patch two
-//     bricks ahead with cp.async; gather each element's 27 values of component c, shift them by
-//     the element's centre value and scale by s_e, apply R^T along the directions where the brick
-//     touches a boundary class, split into TF32 hi/lo and store A_hi into TMEM (row m = element m
-//     = lane m) and A_lo into shared memory, in two A slots;
-//   warp 24 (MMA, one thread): holds B = K_main hi/lo in shared memory and issues the 36
+//     bricks ahead with cp.async; on bricks at the grid's ends transform the patch by E' (the
+//     boundary extraction); gather each element's 27 values of component c, shift them by the
+//     element's centre value and scale by s_e, split into TF32 hi/lo and store A_hi into TMEM
+//     (row m = element m = lane m) and A_lo into shared memory, in two A slots;
+//   warp 24 (MMA, one thread): holds B = K_u hi/lo in shared memory and issues the 36
 //     tcgen05.mma of a brick (A_lo B_hi from shared memory, A_hi B_lo and A_hi B_hi with A from
 //     TMEM) into one of two TMEM accumulators;
 //   warps 12-23 (epilogue, same split): read their 32 accumulator columns with tcgen05.ld and
-//     release them, apply R and sum the element results per patch node with warp shuffles (x, y)
-//     and a shared buffer (z), then write the brick partials.
+//     release them, sum the element results per patch node with warp shuffles (x, y) and a
+//     shared buffer (z), then write the brick partials (the node-side pass applies E).
 // mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full, fin.
 // Every wait is bounded.  On time-out the waiting thread raises a shared abort flag; every other
 // wait then returns false at once.  The builders and the epilogue decide at a barrier that ORs
@@ -132,36 +164,40 @@ struct BrickBox {
     int x0, y0, z0, ex_n, ey_n, ez_n;
 };
 
-// Walks the bricks b, b + step, b + 2 step, ... of a persistent CTA without integer divisions in
-// the loop (the step is split into per-direction increments once).
-struct BrickWalk {
-    int bx, by, bz, sx, sy, sz;
-    __device__ __forceinline__ void init(const Geom &g, int b, int step) {
-        bx = b % g.nbx;
-        by = (b / g.nbx) % g.nby;
-        bz = b / (g.nbx * g.nby);
-        sx = step % g.nbx;
-        sy = (step / g.nbx) % g.nby;
-        sz = step / (g.nbx * g.nby);
+__device__ __forceinline__ BrickBox brick_box(const Geom &g, int local) {
+    const int bx = local % g.nbx, by = (local / g.nbx) % g.nby, bz = local / (g.nbx * g.nby);
+    BrickBox r;
+    r.x0 = bx * kBX;
+    r.y0 = by * kBY;
+    r.z0 = bz * kBZ;
+    r.ex_n = min(kBX, g.nx - r.x0);
+    r.ey_n = min(kBY, g.ny - r.y0);
+    r.ez_n = min(kBZ, g.nz - r.z0);
+    return r;
+}
+
+// The bricks of a persistent CTA: blockIdx.x, blockIdx.x + gridDim.x, ... in the batch's brick
+// numbering, without the bricks of systems whose solve has stopped (their state does not change
+// while the kernel runs, so every role of the CTA walks the same sequence).
+struct BrickCursor {
+    int b, i;   // brick of the batch and its system; b >= nbricks when the walk is over
+    __device__ __forceinline__ void settle(const TcInst *__restrict__ I, int ninst, int nbricks) {
+        while (b < nbricks) {
+            while (i + 1 < ninst && b >= I[i + 1].brick0) ++i;
+            const PcgState *st = I[i].st;
+            if (!st || __ldcg(&st->status) == 0) return;
+            const int end = i + 1 < ninst ? I[i + 1].brick0 : nbricks;
+            b += ((end - b + (int)gridDim.x - 1) / (int)gridDim.x) * (int)gridDim.x;
+        }
     }
-    __device__ __forceinline__ void next(const Geom &g) {
-        bx += sx;
-        const int cy = bx >= g.nbx ? 1 : 0;
-        bx -= cy * g.nbx;
-        by += sy + cy;
-        const int cz = by >= g.nby ? 1 : 0;
-        by -= cz * g.nby;
-        bz += sz + cz;
+    __device__ __forceinline__ void start(const TcInst *__restrict__ I, int ninst, int nbricks) {
+        b = blockIdx.x;
+        i = 0;
+        settle(I, ninst, nbricks);
     }
-    __device__ __forceinline__ BrickBox box(const Geom &g) const {
-        BrickBox r;
-        r.x0 = bx * kBX;
-        r.y0 = by * kBY;
-        r.z0 = bz * kBZ;
-        r.ex_n = min(kBX, g.nx - r.x0);
-        r.ey_n = min(kBY, g.ny - r.y0);
-        r.ez_n = min(kBZ, g.nz - r.z0);
-        return r;
+    __device__ __forceinline__ void next(const TcInst *__restrict__ I, int ninst, int nbricks) {
+        b += gridDim.x;
+        settle(I, ninst, nbricks);
     }
 };
 
@@ -199,20 +235,20 @@ __device__ __forceinline__ void edge_in(float *P, const Edge &E, int o, int ext,
         if (loc[b] >= 0) P[base + loc[b] * stride] = v[b];
 }
 
-__device__ __forceinline__ float row_scale(const Geom &g, const BrickBox &bb, int r, const float *__restrict__ scale) {
+// s_e times the system's K_u factor for brick row r (element lx + 8 ly + 32 lz), 0 outside the grid
+__device__ __forceinline__ float row_scale(const TcInst &I, const BrickBox &bb, int r) {
     const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
     if (lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n)
-        return scale[(long long)(bb.x0 + lx) + (long long)g.nx * ((bb.y0 + ly) + (long long)g.ny * (bb.z0 + lz))];
+        return I.kfac * I.scale[(long long)(bb.x0 + lx) +
+                                (long long)I.g.nx * ((bb.y0 + ly) + (long long)I.g.ny * (bb.z0 + lz))];
     return 0.f;
 }
 
 // 25 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
 // the compiler caps a thread at 72
 __global__ void __launch_bounds__(kPtThreads, 1)
-apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ scale, const float4 *__restrict__ bmat,
-                const Edge *__restrict__ edge, const uint8_t *__restrict__ bflags, float *__restrict__ patch_out,
-                int *__restrict__ err, const PcgState *__restrict__ st) {
-    if (st && st->status != 0) return;
+apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const float4 *__restrict__ bmat,
+                int *__restrict__ err) {
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
     float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
@@ -221,17 +257,19 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
-    __shared__ Edge s_edge;
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
              *fin = bars + 9;
+    {
+        BrickCursor c0;
+        c0.start(insts, ninst, nbricks);
+        if (c0.b >= nbricks) return;   // nothing for this CTA (the same for all its threads)
+    }
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
         tc::tmem_alloc(&tmem_base, kPtTmemCols);
         tc::tmem_relinquish();
     }
-    for (int i = tid; i < int(sizeof(Edge) / 4); i += kPtThreads)
-        reinterpret_cast<int *>(&s_edge)[i] = reinterpret_cast<const int *>(edge)[i];
     if (tid == 0) {
         tc::mbar_init(&a_full[0], kRoleThreads);
         tc::mbar_init(&a_full[1], kRoleThreads);
@@ -250,7 +288,6 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
-    const int nmine = blockIdx.x < g.nbricks ? (g.nbricks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (warp < kRoleWarps) {
         // ------------------------------ builders ------------------------------
@@ -261,14 +298,17 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         // patch rows (c, pz, py) of kPX floats; thread tid < 108 copies row tid, in 8-byte pieces
         // when the row is whole and starts on an even float (always when the x control-point
         // count is even), else float by float
-        auto load_patch = [&](const BrickBox &bb, float *dst) {
-            if (tid < 3 * kPZ * kPY) {
+        auto load_patch = [&](const BrickCursor &cu, float *dst) {
+            if (cu.b < nbricks && tid < 3 * kPZ * kPY) {
+                const TcInst &I = insts[cu.i];
+                const Geom &g = I.g;
+                const BrickBox bb = brick_box(g, cu.b - I.brick0);
                 const int rc = tid / (kPZ * kPY), py = tid % kPY, pz = (tid / kPY) % kPZ;
                 const int gy = bb.y0 + py, gz = bb.z0 + pz;
                 float *drow = dst + tid * kPX;
                 if (gy < g.cy && gz < g.cz) {
                     const long long off = (long long)rc * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
-                    const float *srow = x + off;
+                    const float *srow = I.xin + off;
                     if (bb.x0 + kPX <= g.cx && !(off & 1)) {
 #pragma unroll
                         for (int px = 0; px < kPX; px += 2) tc::cp_async8(drow + px, srow + px);
@@ -286,32 +326,33 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             }
             tc::cp_async_commit();
         };
-        // three patch buffers: brick it + 2 is fetched while brick it is built
-        BrickWalk wc, wl;
-        wc.init(g, blockIdx.x, gridDim.x);
-        wl = wc;
-        if (nmine > 0) load_patch(wl.box(g), sP);
-        else tc::cp_async_commit();
-        wl.next(g);
-        if (nmine > 1) load_patch(wl.box(g), sP + 3 * kPVol);
-        else tc::cp_async_commit();
-        wl.next(g);
-        unsigned fl_next = nmine > 0 ? bflags[blockIdx.x] : 0u;
+        // three patch buffers: the brick two ahead is fetched while one is built
+        BrickCursor cur, ld;
+        cur.start(insts, ninst, nbricks);
+        ld = cur;
+        load_patch(ld, sP);
+        ld.next(insts, ninst, nbricks);
+        load_patch(ld, sP + 3 * kPVol);
+        ld.next(insts, ninst, nbricks);
         const int r = q * 32 + lane;
-        float se_next = nmine > 0 ? row_scale(g, wc.box(g), r, scale) : 0.f;
-        for (int it = 0; it < nmine; ++it, wc.next(g), wl.next(g)) {
+        unsigned fl_next = insts[cur.i].bflags[cur.b - insts[cur.i].brick0];
+        float se_next = row_scale(insts[cur.i], brick_box(insts[cur.i].g, cur.b - insts[cur.i].brick0), r);
+        for (int it = 0; cur.b < nbricks; ++it) {
             const int s = it & 1, pb = it % 3;
             const unsigned fl = fl_next;   // bit d: the brick's patch holds boundary points of d
-            const float se = se_next;      // s_e of this thread's element (0 outside the grid)
-            if (it + 1 < nmine) {
-                fl_next = bflags[blockIdx.x + (it + 1) * gridDim.x];
-                BrickWalk wn1 = wc;
-                wn1.next(g);
-                se_next = row_scale(g, wn1.box(g), r, scale);
+            const float se = se_next;      // s_e k of this thread's element (0 outside the grid)
+            const TcInst &I = insts[cur.i];
+            const Geom &g = I.g;
+            const BrickBox bb = brick_box(g, cur.b - I.brick0);
+            BrickCursor nx = cur;
+            nx.next(insts, ninst, nbricks);
+            if (nx.b < nbricks) {
+                const TcInst &In = insts[nx.i];
+                fl_next = In.bflags[nx.b - In.brick0];
+                se_next = row_scale(In, brick_box(In.g, nx.b - In.brick0), r);
             }
-            if (it + 2 < nmine) load_patch(wl.box(g), sP + ((it + 2) % 3) * 3 * kPVol);
-            else tc::cp_async_commit();
-            const BrickBox bb = wc.box(g);
+            load_patch(ld, sP + ((it + 2) % 3) * 3 * kPVol);
+            ld.next(insts, ninst, nbricks);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const float vm = valid ? se : 0.f;
             tc::cp_async_wait<2>();
@@ -320,16 +361,17 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             if (tc::named_sync_or(1, kRoleThreads, !ok || s_abort != 0)) break;
             if (fl) {   // V = E' u on the boundary control planes, one direction after the other
                 float *P = sP + pb * 3 * kPVol;
+                const Edge &E = *I.edge;
                 if (fl & 1u) {
-                    edge_in<0>(P, s_edge, bb.x0, min(kPX, g.cx - bb.x0), tid);
+                    edge_in<0>(P, E, bb.x0, min(kPX, g.cx - bb.x0), tid);
                     tc::named_sync(1, kRoleThreads);
                 }
                 if (fl & 2u) {
-                    edge_in<1>(P, s_edge, bb.y0, min(kPY, g.cy - bb.y0), tid);
+                    edge_in<1>(P, E, bb.y0, min(kPY, g.cy - bb.y0), tid);
                     tc::named_sync(1, kRoleThreads);
                 }
                 if (fl & 4u) {
-                    edge_in<2>(P, s_edge, bb.z0, min(kPZ, g.cz - bb.z0), tid);
+                    edge_in<2>(P, E, bb.z0, min(kPZ, g.cz - bb.z0), tid);
                     tc::named_sync(1, kRoleThreads);
                 }
             }
@@ -364,6 +406,7 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             tc::fence_before_sync();
             tc::mbar_arrive(&a_full[s]);
             tc::named_sync(1, kRoleThreads);   // everyone is done with this patch before it is refilled
+            cur = nx;
         }
         tc::cp_async_wait<0>();
     } else if (warp < 2 * kRoleWarps) {
@@ -390,8 +433,9 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             zb[k] = 9 * (kPY * kPX) * pz + (kPY * kPX) * ci + pyx;
             zpz[k] = pz;
         }
-        for (int it = 0; it < nmine; ++it) {
-            const int b = blockIdx.x + it * gridDim.x;
+        BrickCursor cur;
+        cur.start(insts, ninst, nbricks);
+        for (int it = 0; cur.b < nbricks; ++it, cur.next(insts, ninst, nbricks)) {
             float *sZ = sZb + (it & 1) * kZFl;
             const int db = it & 1;
             // on a failed wait the values read below are not used: the barrier before the z-sum
@@ -432,11 +476,11 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
                     const float y4 = fmaf(my1, t1, a1);
                     const int px = var == 0 ? lx : 7 + var;
                     if (var == 0 || lx == 7) {
-                        float *zb = sZ + (((q * 3 + az) * 3 + c) * kPY) * kPX + px;
-                        zb[ly * kPX] = yv;
+                        float *zp = sZ + (((q * 3 + az) * 3 + c) * kPY) * kPX + px;
+                        zp[ly * kPX] = yv;
                         if (ly == 3) {
-                            zb[4 * kPX] = y4;
-                            zb[5 * kPX] = a2;
+                            zp[4 * kPX] = y4;
+                            zp[5 * kPX] = a2;
                         }
                     }
                 }
@@ -444,7 +488,8 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
             // the other buffer) finished before its thread reached this barrier
             if (tc::named_sync_or(2, kRoleThreads, !ok || s_abort != 0)) break;
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
-            float *ob = patch_out + (size_t)b * 3 * kPVol + et;
+            const TcInst &I = insts[cur.i];
+            float *ob = I.patch + (size_t)(cur.b - I.brick0) * 3 * kPVol + et;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 if (et + k * kRoleThreads >= 3 * kPVol) break;
@@ -466,8 +511,11 @@ apply_tc_kernel(Geom g, const float *__restrict__ x, const float *__restrict__ s
         // so adding a step's offset never carries out of the address field
         const uint64_t dbh0 = tc::make_desc(sB, kBLbo, kSbo), dbl0 = tc::make_desc(sB + kBFl, kBLbo, kSbo);
         const uint64_t dal0 = tc::make_desc(sAlo, kALbo, kSbo), dal1 = tc::make_desc(sAlo + kAloFl, kALbo, kSbo);
-        for (int it = 0; it < nmine && run; ++it) {
-            const int s = it & 1, db = it & 1;
+        BrickCursor cur;
+        cur.start(insts, ninst, nbricks);
+        int nmine = 0;   // bricks issued
+        for (; cur.b < nbricks && run; cur.next(insts, ninst, nbricks), ++nmine) {
+            const int it = nmine, s = it & 1, db = it & 1;
             // slot s holds brick it, and brick it - 2 has been drained from accumulator buffer db;
             // on a failed wait nothing more is issued
             run = pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err) &&
@@ -587,6 +635,16 @@ __device__ bool grid_sync(unsigned long long *ctr, int *err, long long limit) {
     return s_ok != 0;
 }
 
+// Arrival at the grid barrier by a CTA that has nothing after it (its system has stopped): the
+// others still count it.
+__device__ void grid_arrive(unsigned long long *ctr) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctr, 1ull);
+    }
+}
+
 // Deterministic block reduction of five values at once; the sums are valid in thread 0.
 __device__ __forceinline__ void block_sum5(double (&v)[5]) {
     __shared__ double ws[5][kTailThreads / 32];
@@ -607,12 +665,13 @@ __device__ __forceinline__ void block_sum5(double (&v)[5]) {
 }
 
 // One launch for everything of a PCG iteration after the operator (rust/src/solver.rs:38-71),
-// with one grid-wide barrier.
+// with one grid-wide barrier, for every system of the batch: system i is served by CTAs
+// [cta0, cta0 + ncta) and reduces its own partials.
 //   Phase A, node by node: Ap = the node sum of the brick partials (with the boundary extraction)
 //   plus the sparse term, output rule applied; and five dot products p'Ap, z'Ap, Ap'D^-1 Ap, r'Ap,
 //   Ap'Ap (z = D^-1 r).
-//   Barrier.  Every CTA reduces the same partials in the same order: alpha = r'z / p'Ap, and for
-//   r_new = r - alpha Ap, without another reduction,
+//   Barrier.  Every CTA of the system reduces the same partials in the same order: alpha =
+//   r'z / p'Ap, and for r_new = r - alpha Ap, without another reduction,
 //       |r_new|^2 = r'r - 2 alpha r'Ap + alpha^2 Ap'Ap,
 //       r_new' D^-1 r_new = r'z - 2 alpha z'Ap + alpha^2 Ap'D^-1 Ap,
 //   which give the convergence test and beta = r_new'z_new / r'z.  When the FP32 residual has
@@ -621,20 +680,36 @@ __device__ __forceinline__ void block_sum5(double (&v)[5]) {
 //   Phase B: x += alpha p, r -= alpha Ap, p = D^-1 r + beta p (when the iteration goes on), and the
 //   exact r'r and r'z of the new r as per-CTA partials, which the next launch reduces in place of
 //   the formulas (so they bridge one iteration only).
-// CTA 0 writes the state.  All CTAs take the same branches.
+// The system's first CTA writes its state.  All CTAs of a system take the same branches; the CTAs
+// of a stopped system only arrive at the barrier.
 __global__ void __launch_bounds__(kTailThreads)
-pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict__ edge, const uint8_t *__restrict__ mask,
-                int mask_mode, Sparse<float> sp, const float *__restrict__ inv, float *__restrict__ x,
-                float *__restrict__ r, float *__restrict__ p, float *__restrict__ pm, float *__restrict__ ap,
-                double *__restrict__ part, PcgState *st, unsigned long long *ctr, int *err, long long wait_limit) {
+pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long *ctr, int *err, long long wait_limit) {
     __shared__ PcgState S;
     __shared__ double s_ab[2];
-    __shared__ int s_stat;
-    if (threadIdx.x == 0) S = *st;
+    __shared__ int s_stat, s_inst;
+    if (threadIdx.x == 0) {
+        int i = 0;
+        while (i + 1 < ninst && (int)blockIdx.x >= insts[i + 1].cta0) ++i;
+        s_inst = i;
+        S = *insts[i].st;
+    }
     __syncthreads();
-    if (S.status != 0) return;
-    const int G = gridDim.x;
-    double *pa = part, *pb = part + 5 * G;   // phase A partials [5][G], exact r'r, r'z [2][G]
+    const TcInst &I = insts[s_inst];
+    if (S.status != 0 || (int)blockIdx.x >= I.cta0 + I.ncta) {
+        grid_arrive(ctr);
+        return;
+    }
+    const Geom g = I.g;
+    const int G = I.ncta, bid = (int)blockIdx.x - I.cta0;
+    const uint8_t *__restrict__ mask = I.mask;
+    const int mask_mode = I.mask_mode;
+    const float *__restrict__ inv = I.inv;
+    float *__restrict__ x = I.x;
+    float *__restrict__ r = I.r;
+    float *__restrict__ p = I.p;
+    float *__restrict__ pm = I.pm;
+    float *__restrict__ ap = I.ap;
+    double *pa = I.part, *pb = I.part + 5 * G;   // phase A partials [5][G], exact r'r, r'z [2][G]
     // exact r'r and r'z of the current r: from the state after an initialisation or replacement,
     // else from the previous launch's phase B
     double rr0 = S.rr_old, rz0 = S.rz_old;
@@ -649,11 +724,11 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict_
         rz0 = v[1];
     }
     const long long T = (long long)G * blockDim.x;
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t0 = (long long)bid * blockDim.x + threadIdx.x;
     const long long n = 3 * g.nsc;
     // A. Ap at every node and the five dot products
     double dA[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const Edge *E = edge && (edge->nb[0] | edge->nb[1] | edge->nb[2]) ? edge : nullptr;
+    const Edge *E = I.edge && (I.edge->nb[0] | I.edge->nb[1] | I.edge->nb[2]) ? I.edge : nullptr;
     // 32-bit index arithmetic: the set-up checks nsc < 2^31
     const unsigned ucx = (unsigned)g.cx, ucy = (unsigned)g.cy;
     for (long long nd = t0; nd < g.nsc; nd += T) {
@@ -662,13 +737,13 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict_
         float sv[3];
         const int sx = E ? edge_slot(*E, 0, ix) : -1, sy = E ? edge_slot(*E, 1, iy) : -1,
                   sz = E ? edge_slot(*E, 2, iz) : -1;
-        if (sx < 0 && sy < 0 && sz < 0) node_partials(g, patch, ix, iy, iz, sv[0], sv[1], sv[2]);
-        else edge_node(g, *E, patch, ix, iy, iz, sx, sy, sz, sv);
+        if (sx < 0 && sy < 0 && sz < 0) node_partials(g, I.patch, ix, iy, iz, sv[0], sv[1], sv[2]);
+        else edge_node(g, *E, I.patch, ix, iy, iz, sx, sy, sz, sv);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const long long idx = (long long)c * g.nsc + nd;
             float v = sv[c];
-            if (sp.ptr) v += sparse_row(sp, idx, p, mask, mask_mode);
+            if (I.sp.ptr) v += sparse_row(I.sp, idx, p, mask, mask_mode);
             if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.f;
             else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
             ap[idx] = v;
@@ -684,7 +759,7 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict_
     block_sum5(dA);
     if (threadIdx.x == 0)
 #pragma unroll
-        for (int k = 0; k < 5; ++k) pa[k * G + blockIdx.x] = dA[k];
+        for (int k = 0; k < 5; ++k) pa[k * G + bid] = dA[k];
     if (!grid_sync(ctr, err, wait_limit)) return;
     {
         double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -722,7 +797,7 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict_
             s_stat = S.status;
             s_ab[0] = S.alpha;
             s_ab[1] = S.beta;
-            if (blockIdx.x == 0) *st = S;
+            if (bid == 0) *I.st = S;
         }
     }
     __syncthreads();
@@ -751,8 +826,8 @@ pcg_tail_kernel(Geom g, const float *__restrict__ patch, const Edge *__restrict_
     }
     block_sum5(v);
     if (threadIdx.x == 0) {
-        pb[blockIdx.x] = v[0];
-        pb[G + blockIdx.x] = v[1];
+        pb[bid] = v[0];
+        pb[G + bid] = v[1];
     }
 }
 
@@ -961,19 +1036,43 @@ static int setup_edge(const Op &op, Edge &edge, std::vector<double> &kunif) {
     return ICC_OK;
 }
 
+static int vecset_alloc(const Op &op, VecSet &v, int part_cap) {
+    const size_t n = (size_t)op.ndof;
+    int rc;
+    if ((rc = dalloc(&v.patch32, (size_t)op.g.nbricks * 3 * kPVol, "alloc mixed"))) return rc;
+    float **f32[] = {&v.rhs32, &v.x32, &v.r32, &v.p32, &v.ap32, &v.xm32, &v.inv32};
+    for (float **p : f32)
+        if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
+    double **f64[] = {&v.x64, &v.r64, &v.y64};
+    for (double **p : f64)
+        if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
+    if ((rc = dalloc(&v.part, (size_t)7 * part_cap, "alloc mixed"))) return rc;
+    v.part_cap = part_cap;
+    return ICC_OK;
+}
+
+static void vecset_free(VecSet &v) {
+    void *bufs[] = {v.patch32, v.rhs32, v.x32, v.r32, v.p32, v.ap32, v.xm32, v.inv32, v.x64, v.r64, v.y64, v.part};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    v = VecSet();
+}
+
+// CTAs of the fused vector step that can be resident at once (its grid barrier needs all of them)
+static int tail_capacity(const Op &op) { return op.mixed->tail_per_sm * op.num_sms; }
+
 static int mixed_init(Op &op) {
     if (op.mixed && op.mixed->ready) return ICC_OK;
     if (op.g.nsc >= (1LL << 31)) return set_error(ICC_BAD_ARG, "tensor-core path: more than 2^31 control points");
     if (!op.mixed) op.mixed = new MixedState();
     MixedState &ms = *op.mixed;
-    std::vector<double> kunif;
-    int rc = setup_edge(op, ms.edge, kunif);
+    int rc = setup_edge(op, ms.edge, ms.kunif);
     if (rc) return rc;
     // the uniform element matrix split into TF32 hi/lo in the canonical layout, component c of
     // the test (row) and trial (column) DOFs at c*32 + [0, 27)
     std::vector<float> bm((size_t)2 * kBFl, 0.f);
     {
-        const double *K = kunif.data();
+        const double *K = ms.kunif.data();
         float *hi = bm.data(), *lo = hi + kBFl;
         for (int n = 0; n < 81; ++n)
             for (int k = 0; k < 81; ++k) {
@@ -1006,34 +1105,24 @@ static int mixed_init(Op &op) {
         ICC_CUDA(cudaMemcpyAsync(ms.d_edge, &ms.edge, sizeof(Edge), cudaMemcpyHostToDevice, op.stream), "copy edge");
         ICC_CUDA(cudaStreamSynchronize(op.stream), "copy brick flags");
     }
-    const size_t n = (size_t)op.ndof;
-    if ((rc = dalloc(&ms.d_scale32, (size_t)op.nel, "alloc mixed"))) return rc;
-    if ((rc = dalloc(&ms.d_patch32, (size_t)g.nbricks * 3 * kPVol, "alloc mixed"))) return rc;
-    float **f32[] = {&ms.d_rhs32, &ms.d_x32, &ms.d_r32, &ms.d_p32, &ms.d_ap32, &ms.d_inv32, &ms.d_xm32};
-    for (float **p : f32)
-        if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
-    double **f64[] = {&ms.d_x64, &ms.d_r64, &ms.d_y64};
-    for (double **p : f64)
-        if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
-    if ((rc = dalloc(&ms.d_scalars, 8, "alloc mixed"))) return rc;
     {
         int per_sm = 0;
         ICC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_tail_kernel, kTailThreads, 0),
                  "tail occupancy");
-        // every CTA must be resident (grid barriers); small grids take only the CTAs they need, so
-        // the fused steps of concurrent solves (icc_pcg_solve_batched) can share the GPU
-        const long long need = (op.g.nsc + kTailThreads - 1) / kTailThreads;
-        ms.tail_grid = (int)std::max(1LL, std::min<long long>((long long)std::max(1, std::min(per_sm, 4)) * op.num_sms, need));
-        if ((rc = dalloc(&ms.d_tail_part, (size_t)7 * ms.tail_grid, "alloc mixed"))) return rc;
-        if ((rc = dalloc(&ms.d_grid_ctr, 1, "alloc mixed"))) return rc;
-        ICC_CUDA(cudaMemsetAsync(ms.d_grid_ctr, 0, sizeof(unsigned long long), op.stream), "clear grid counter");
+        ms.tail_per_sm = std::max(1, std::min(per_sm, 4));
     }
+    if ((rc = dalloc(&ms.d_scale32, (size_t)op.nel, "alloc mixed"))) return rc;
+    if ((rc = vecset_alloc(op, ms.v, tail_capacity(op)))) return rc;
+    if ((rc = dalloc(&ms.d_scalars, 8, "alloc mixed"))) return rc;
+    if ((rc = dalloc(&ms.d_grid_ctr, 1, "alloc mixed"))) return rc;
     if ((rc = dalloc(&ms.d_err, 1, "alloc mixed"))) return rc;
     if ((rc = dalloc(&ms.d_state, 1, "alloc mixed"))) return rc;
+    if ((rc = dalloc(&ms.d_inst, 2, "alloc mixed"))) return rc;   // [0] plain apply, [1] the handle's solve
     ICC_CUDA(cudaMallocHost((void **)&ms.h_state, sizeof(PcgState)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&ms.h_scalars, 8 * sizeof(double)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&ms.h_err, sizeof(int)), "alloc pinned");
     ICC_CUDA(cudaMemsetAsync(ms.d_err, 0, sizeof(int), op.stream), "clear err");
+    ICC_CUDA(cudaMemsetAsync(ms.d_grid_ctr, 0, sizeof(unsigned long long), op.stream), "clear grid counter");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "clear err");
     ICC_CUDA(cudaFuncSetAttribute(apply_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPtSmem),
              "cudaFuncSetAttribute tc");
@@ -1045,9 +1134,9 @@ void mixed_release(Op &op) {
     if (!op.mixed) return;
     MixedState &ms = *op.mixed;
     if (ms.graph) cudaGraphExecDestroy(ms.graph);
-    void *bufs[] = {ms.d_bmat, ms.d_bflags, ms.d_edge, ms.d_scale32, ms.d_patch32, ms.d_rhs32, ms.d_x32, ms.d_r32, ms.d_p32,
-                    ms.d_ap32, ms.d_inv32, ms.d_xm32, ms.d_x64, ms.d_r64, ms.d_y64, ms.d_scalars,
-                    ms.d_err, ms.d_state, ms.d_tail_part, ms.d_grid_ctr};
+    vecset_free(ms.v);
+    void *bufs[] = {ms.d_bmat, ms.d_bflags, ms.d_edge, ms.d_scale32, ms.d_scalars, ms.d_err, ms.d_state,
+                    ms.d_grid_ctr, ms.d_inst};
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (ms.h_state) cudaFreeHost(ms.h_state);
@@ -1072,58 +1161,81 @@ __global__ void mask_copy_kernel(long long n, const float *__restrict__ x, const
         xm[i] = mask[i] ? x[i] : 0.f;
 }
 
-static void launch_apply_tc(Op &op, const float *xin, const PcgState *st) {
-    MixedState &ms = *op.mixed;
-    const int grid = std::min(op.num_sms, op.g.nbricks);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, op.stream>>>(op.g, xin, ms.d_scale32, ms.d_bmat, ms.d_edge,
-                                                              ms.d_bflags, ms.d_patch32, ms.d_err, st);
+// The instance entry of system (op, v) with PCG state st (null: a plain apply of xin).
+static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, const float *xin, int brick0, int cta0, int ncta,
+                        float kfac) {
+    const MixedState &ms = *op.mixed;
+    const bool ident = op.mask_mode == ICC_MASK_IDENTITY;
+    TcInst I;
+    std::memset(&I, 0, sizeof(I));
+    I.g = op.g;
+    I.brick0 = brick0;
+    I.cta0 = cta0;
+    I.ncta = ncta;
+    I.kfac = kfac;
+    I.xin = xin ? xin : (ident ? v.xm32 : v.p32);
+    I.scale = ms.d_scale32;
+    I.bflags = ms.d_bflags;
+    I.edge = ms.d_edge;
+    I.patch = v.patch32;
+    I.mask = op.mask_mode != ICC_MASK_NONE ? op.d_mask : nullptr;
+    I.mask_mode = op.mask_mode;
+    I.sp = op.extra32();
+    I.inv = v.inv32;
+    I.x = v.x32;
+    I.r = v.r32;
+    I.p = v.p32;
+    I.pm = ident ? v.xm32 : nullptr;
+    I.ap = v.ap32;
+    I.part = v.part;
+    I.st = st;
+    return I;
+}
+
+static void launch_apply_tc(cudaStream_t s, const TcInst *d_insts, int ninst, int nbricks, const float4 *bmat, int *err,
+                            int num_sms) {
+    const int grid = std::min(num_sms, nbricks);
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, s>>>(d_insts, ninst, nbricks, bmat, err);
+}
+
+static cudaError_t launch_tail(cudaStream_t s, const TcInst *d_insts, int ninst, int grid, unsigned long long *ctr,
+                               int *err, long long limit) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;   // the grid barrier needs every CTA resident
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, pcg_tail_kernel, d_insts, ninst, ctr, err, limit);
 }
 
 // enqueue y32 = A x32 with the tensor-core apply; a masked operator first zeroes the fixed DOFs of
 // the input (into the xm32 scratch vector), the node-side pass applies the output rule
-static void enqueue_apply_tc(Op &op, const float *x, float *y) {
+static int enqueue_apply_tc(Op &op, const float *x, float *y) {
     MixedState &ms = *op.mixed;
     const float *xin = x;
     if (op.mask_mode != ICC_MASK_NONE) {
-        mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.ndof, x, op.d_mask, ms.d_xm32);
-        xin = ms.d_xm32;
+        mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.ndof, x, op.d_mask, ms.v.xm32);
+        xin = ms.v.xm32;
     }
-    launch_apply_tc(op, xin, nullptr);
-    gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, ms.d_edge, x, op.d_mask,
-                                                                       op.mask_mode,
-                                                                       op.extra32(), y, nullptr, nullptr);
-}
-
-// One iteration of the FP32 PCG: the tensor-core apply and the fused vector step.  With
-// ICC_MASK_ZERO the search direction is kept zero on fixed DOFs; with ICC_MASK_IDENTITY the
-// direction update also writes the masked copy the brick apply reads.
-static cudaError_t enqueue_inner_iteration(Op &op) {
-    MixedState &ms = *op.mixed;
-    const bool zero = op.mask_mode == ICC_MASK_ZERO, ident = op.mask_mode == ICC_MASK_IDENTITY;
-    launch_apply_tc(op, ident ? ms.d_xm32 : ms.d_p32, ms.d_state);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)ms.tail_grid);
-    cfg.blockDim = dim3(kTailThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = op.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;   // the grid barriers need every CTA resident
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pcg_tail_kernel, op.g, (const float *)ms.d_patch32, (const Edge *)ms.d_edge,
-                              (const uint8_t *)(zero || ident ? op.d_mask : nullptr), op.mask_mode, op.extra32(),
-                              (const float *)ms.d_inv32, ms.d_x32, ms.d_r32, ms.d_p32, ident ? ms.d_xm32 : nullptr,
-                              ms.d_ap32, ms.d_tail_part, ms.d_state, ms.d_grid_ctr, ms.d_err,
-                              ms.grid_wait_limit);
+    const TcInst I = make_inst(op, ms.v, nullptr, xin, 0, 0, 0, 1.f);
+    ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
+    launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_bmat, ms.d_err, op.num_sms);
+    gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, ms.d_edge, x, op.d_mask,
+                                                                       op.mask_mode, op.extra32(), y, nullptr, nullptr);
+    ICC_CUDA(cudaGetLastError(), "tc apply launch");
+    return ICC_OK;
 }
 
 // Clears the device error flag and the grid-barrier counter before a call, so a handle whose
 // previous call timed out starts clean (stream-ordered before the call's kernels).
-static int clear_flags(Op &op) {
-    MixedState &ms = *op.mixed;
-    ICC_CUDA(cudaMemsetAsync(ms.d_err, 0, sizeof(int), op.stream), "clear err");
-    ICC_CUDA(cudaMemsetAsync(ms.d_grid_ctr, 0, sizeof(unsigned long long), op.stream), "clear grid counter");
+static int clear_flags(cudaStream_t s, int *d_err, unsigned long long *d_ctr) {
+    ICC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s), "clear err");
+    ICC_CUDA(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned long long), s), "clear grid counter");
     return ICC_OK;
 }
 
@@ -1136,13 +1248,12 @@ static int timeout_error(int err) {
 int mixed_apply_f32(Op &op, const float *x, float *y) {
     int rc = mixed_init(op);
     if (rc) return rc;
-    if ((rc = clear_flags(op))) return rc;
-    enqueue_apply_tc(op, x, y);
-    ICC_CUDA(cudaGetLastError(), "tc apply launch");
-    int err = 0;
-    ICC_CUDA(cudaMemcpyAsync(&err, op.mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
+    MixedState &ms = *op.mixed;
+    if ((rc = clear_flags(op.stream, ms.d_err, ms.d_grid_ctr))) return rc;
+    if ((rc = enqueue_apply_tc(op, x, y))) return rc;
+    ICC_CUDA(cudaMemcpyAsync(ms.h_err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "tc apply");
-    if (err) return timeout_error(err);
+    if (*ms.h_err) return timeout_error(*ms.h_err);
     return ICC_OK;
 }
 
@@ -1166,15 +1277,17 @@ int mixed_set_wait_limit(Op &op, long long polls) {
 int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *contract_ms, double *gather_ms) {
     int rc = mixed_init(op);
     if (rc) return rc;
-    if ((rc = clear_flags(op))) return rc;
     MixedState &ms = *op.mixed;
+    if ((rc = clear_flags(op.stream, ms.d_err, ms.d_grid_ctr))) return rc;
+    const TcInst I = make_inst(op, ms.v, nullptr, x, 0, 0, 0, 1.f);
+    ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
     std::vector<cudaEvent_t> ev(3 * size_t(reps));
     for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(ev[3 * r], op.stream);
-        launch_apply_tc(op, x, nullptr);
+        launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_bmat, ms.d_err, op.num_sms);
         cudaEventRecord(ev[3 * r + 1], op.stream);
-        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.d_patch32, ms.d_edge, x, op.d_mask,
+        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, ms.d_edge, x, op.d_mask,
                                                                            ICC_MASK_NONE, op.extra32(), y, nullptr,
                                                                            nullptr);
         cudaEventRecord(ev[3 * r + 2], op.stream);
@@ -1190,10 +1303,9 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     }
     for (auto &x2 : ev) cudaEventDestroy(x2);
     ICC_CUDA(e, "profile tc apply");
-    int err = 0;
-    ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
+    ICC_CUDA(cudaMemcpyAsync(ms.h_err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
     ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
-    if (err) return timeout_error(err);
+    if (*ms.h_err) return timeout_error(*ms.h_err);
     *contract_ms = a / reps;
     *gather_ms = gt / reps;
     return ICC_OK;
@@ -1247,158 +1359,429 @@ ru_replace_finalize(const double *__restrict__ partials, int np, PcgState *st) {
     }
 }
 
-// Mixed-precision PCG with reliable updates (residual replacement): the Jacobi-PCG recurrence runs
-// in FP32 on the tensor-core operator; whenever its residual has fallen by `delta` since the last
-// replacement (or below tol), the FP32 solution increment is folded into the FP64 solution, the
-// true residual b - A x is recomputed with the FP64 operator, and the FP32 residual is replaced by
-// it while the search direction is kept.  Stops when the FP64 residual meets tol (the reference's
-// stopping rule, rust/src/solver.rs:56-58, evaluated on the true residual).
-int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter, const icc_solve_opts &opts,
-                double *x_out, int64_t *iters, double *rel_res) {
-    int rc = op.ensure_pcg_buffers();
-    if (rc) return rc;
-    if ((rc = mixed_init(op))) return rc;
-    if ((rc = clear_flags(op))) return rc;
-    MixedState &ms = *op.mixed;
-    const int vb = op.vec_blocks;
-    const long long n = op.ndof;
+// ---- the mixed-precision solve of one or several systems ------------------------------------
+
+// Per-system inputs, outputs and loop state of a (batched) mixed solve.
+struct MixedItem {
+    Op *op = nullptr;
+    VecSet *v = nullptr;
+    const double *b = nullptr, *diag = nullptr;
+    double tol = 0.0;
+    int64_t max_iter = 0;
+    double *x_out = nullptr;
+    float kfac = 1.f;
+    // results
+    int status = ICC_NOT_CONVERGED;
+    int64_t iters = 0, updates = 0;
+    double rel_res = 1.0;
+    // loop state
+    double nb = 1.0, res = 1.0, best = INFINITY;
+    int no_progress = 0;
+    bool done = false;
+};
+
+// The device side of a (batched) mixed solve: the instance table, the systems' states (one
+// array, read back with one copy per graph batch) and the captured iteration graph.
+struct MixedBatch {
+    cudaStream_t stream = nullptr;
+    TcInst *d_inst = nullptr;
+    PcgState *d_state = nullptr, *h_state = nullptr;
+    double *d_scalars = nullptr, *h_scalars = nullptr;   // |b|^2 and |r|^2 per system
+    int *d_err = nullptr, *h_err = nullptr;
+    unsigned long long *d_ctr = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int ninst = 0, nbricks = 0, tail_grid = 0, num_sms = 148;
+    const float4 *bmat = nullptr;
+    long long limit = kGridWaitLimit;
+    bool owned = false;   // allocated for this call (a batch), else borrowed from the handle
+    ~MixedBatch() {
+        if (!owned) return;
+        if (graph) cudaGraphExecDestroy(graph);
+        void *bufs[] = {d_inst, d_state, d_scalars, d_err, d_ctr};
+        for (void *p : bufs)
+            if (p) cudaFree(p);
+        if (h_state) cudaFreeHost(h_state);
+        if (h_scalars) cudaFreeHost(h_scalars);
+        if (h_err) cudaFreeHost(h_err);
+    }
+};
+
+// Shares the fused vector step's CTAs among the systems: every system gets at least one, the
+// rest in proportion to its control points (no more than one per 256 of them).
+static std::vector<int> share_ctas(const std::vector<MixedItem> &items, int cap) {
+    const size_t m = items.size();
+    std::vector<int> n(m, 1);
+    long long tot = 0;
+    for (const auto &it : items) tot += it.op->g.nsc;
+    int used = int(m);
+    for (size_t i = 0; i < m; ++i) {
+        const long long need = (items[i].op->g.nsc + kTailThreads - 1) / kTailThreads;
+        const long long want = (long long)((double)(cap - (int)m) * (double)items[i].op->g.nsc / (double)tot);
+        const int add = (int)std::max(0LL, std::min(need - 1, want));
+        n[i] += add;
+        used += add;
+    }
+    (void)used;
+    return n;
+}
+
+// Runs the graph batches of a (batched) mixed solve until every system has stopped.
+//
+// Reliable-update PCG per system: the Jacobi-PCG recurrence runs in FP32 on the tensor-core
+// operator; whenever its residual has fallen by `delta` since the last replacement (or below tol),
+// the FP32 solution increment is folded into the FP64 solution, the true residual b - A x is
+// recomputed with the FP64 operator, and the FP32 residual is replaced by it while the search
+// direction is kept.  A system stops when its FP64 residual meets its tolerance (the reference's
+// stopping rule, rust/src/solver.rs:56-58, evaluated on the true residual), on breakdown or NaN,
+// or when its iteration budget or progress runs out.
+static int run_mixed(MixedBatch &bt, std::vector<MixedItem> &items, const icc_solve_opts &opts, int64_t *launches_out) {
+    cudaStream_t s = bt.stream;
+    const size_t m = items.size();
     // 0.6: a replacement every ~75 iterations at 128x64x64 keeps the FP32 recurrence close to the
     // FP64 iteration count (1,350-1,410 vs 1,337 over four seeds; 0.1 gave up to 1,820)
     const double delta = opts.inner_tol > 0.0 ? opts.inner_tol : 0.6;
     const int max_updates = opts.max_outer > 0 ? opts.max_outer : 1000;
     const int check_every = opts.check_every > 0 ? opts.check_every : 32;
-    const uint8_t *pm = op.mask_mode == ICC_MASK_ZERO ? op.d_mask : nullptr;
-    int64_t launches = 0;
-
-    if (!diag) {
-        if ((rc = op.diagonal_dev(op.d_diag))) return rc;
-        diag = op.d_diag;
-        launches++;
-    }
-    inv_diag_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(n, diag, ms.d_inv32);
-    ir_init_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, b, ms.d_x64, ms.d_r64, op.d_partials);
-    sum_partials_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_scalars, 0);
-    launches += 3;
-    ICC_CUDA(cudaMemcpyAsync(ms.h_scalars, ms.d_scalars, 8, cudaMemcpyDeviceToHost, op.stream), "scalars");
-    ICC_CUDA(cudaStreamSynchronize(op.stream), "mixed init");
-    const double nb = std::fmax(std::sqrt(ms.h_scalars[0]), 1e-16);
-    const double sigma = nb;  // FP32 quantities are scaled by 1 / |b|
-    if (max_iter == 0) {
-        ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
-        *iters = 0;
-        *rel_res = 1.0;
-        return ICC_NOT_CONVERGED;
-    }
-    ir_to_f32_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r64, ms.d_rhs32, ms.d_scalars);
-    pcg_init_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_rhs32, ms.d_inv32, ms.d_x32, ms.d_r32, ms.d_p32,
-                                                              op.d_partials, pm);
-    pcg_init_finalize<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state, tol, (long long)max_iter);
     constexpr int64_t kMaxSegment = 512;  // FP32 iterations between residual replacements at most
-    ru_arm_kernel<<<1, 1, 0, op.stream>>>(ms.d_state, 1.0, delta, kMaxSegment, check_every);
-    launches += 4;
-    if (op.mask_mode == ICC_MASK_IDENTITY) {
-        mask_copy_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_p32, op.d_mask, ms.d_xm32);
-        launches++;
-    }
-
-    if (!ms.graph || ms.graph_batch != check_every || ms.graph_limit != ms.grid_wait_limit) {
-        if (ms.graph) cudaGraphExecDestroy(ms.graph);
-        ms.graph = nullptr;
-        cudaGraph_t graph;
-        ICC_CUDA(cudaStreamBeginCapture(op.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        cudaError_t ce = cudaSuccess;
-        for (int i = 0; i < check_every && ce == cudaSuccess; ++i) ce = enqueue_inner_iteration(op);
-        cudaError_t ee = cudaStreamEndCapture(op.stream, &graph);
-        ICC_CUDA(ce, "capture fused vector step");
-        ICC_CUDA(ee, "end capture");
-        cudaError_t e = cudaGraphInstantiate(&ms.graph, graph, 0);
-        cudaGraphDestroy(graph);
-        ICC_CUDA(e, "graph instantiate");
-        ms.graph_batch = check_every;
-        ms.graph_limit = ms.grid_wait_limit;
-    }
-
-    int status = ICC_NOT_CONVERGED;
-    int64_t updates = 0, launched = 0;
-    double res = 1.0, best = INFINITY;
-    int no_progress = 0;
     // give up after the FP32 recurrence has gained eight decades (8 ln 0.1 / ln delta replacements)
     // without a 10% improvement of the true residual
     const int max_no_progress = std::max(8, (int)std::ceil(8.0 * std::log(0.1) / std::log(std::fmin(delta, 0.99))));
-    for (;;) {
-        ICC_CUDA(cudaGraphLaunch(ms.graph, op.stream), "graph launch");
+    int64_t launches = 0;
+    int rc;
+    if ((rc = clear_flags(s, bt.d_err, bt.d_ctr))) return rc;
+    // initialisation: x = 0, r = b, |b| per system
+    for (size_t i = 0; i < m; ++i) {
+        MixedItem &it = items[i];
+        Op &op = *it.op;
+        VecSet &v = *it.v;
+        const double *diag = it.diag;
+        if (!diag) {
+            op.enqueue_diagonal(op.d_diag, s);
+            diag = op.d_diag;
+            launches++;
+        }
+        inv_diag_kernel<float><<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, diag, v.inv32);
+        ir_init_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, it.b, v.x64, v.r64, op.d_partials);
+        sum_partials_kernel<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_scalars, (int)i);
+        launches += 3;
+    }
+    ICC_CUDA(cudaMemcpyAsync(bt.h_scalars, bt.d_scalars, m * sizeof(double), cudaMemcpyDeviceToHost, s), "scalars");
+    ICC_CUDA(cudaStreamSynchronize(s), "mixed init");
+    for (size_t i = 0; i < m; ++i) {
+        MixedItem &it = items[i];
+        Op &op = *it.op;
+        VecSet &v = *it.v;
+        it.nb = std::fmax(std::sqrt(bt.h_scalars[i]), 1e-16);   // FP32 quantities are scaled by 1 / |b|
+        if (it.max_iter == 0) {
+            it.done = true;
+            it.status = ICC_NOT_CONVERGED;
+            it.rel_res = 1.0;
+            // a stopped state, so the kernels skip the system
+            ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, 1.0, 0.0, kMaxSegment, check_every);
+            pcg_init_finalize<<<1, kVecThreads, 0, s>>>(op.d_partials, 0, bt.d_state + i, it.tol, 0);
+            launches += 2;
+            continue;
+        }
+        const uint8_t *pm = op.mask_mode == ICC_MASK_ZERO ? op.d_mask : nullptr;
+        ir_to_f32_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.r64, v.rhs32, bt.d_scalars + i);
+        pcg_init_kernel<float><<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.rhs32, v.inv32, v.x32, v.r32, v.p32,
+                                                                     op.d_partials, pm);
+        pcg_init_finalize<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_state + i, it.tol,
+                                                    (long long)it.max_iter);
+        ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, 1.0, delta, kMaxSegment, check_every);
+        launches += 4;
+        if (op.mask_mode == ICC_MASK_IDENTITY) {
+            mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.p32, op.d_mask, v.xm32);
+            launches++;
+        }
+    }
+    ICC_CUDA(cudaGetLastError(), "mixed init");
+
+    int64_t launched = 0, max_budget = 0;
+    for (const auto &it : items) max_budget = std::max(max_budget, it.max_iter);
+    size_t active = 0;
+    for (const auto &it : items) active += it.done ? 0 : 1;
+    while (active > 0) {
+        ICC_CUDA(cudaGraphLaunch(bt.graph, s), "graph launch");
         launches += 2 * int64_t(check_every);
         launched += check_every;
-        ICC_CUDA(cudaMemcpyAsync(ms.h_state, ms.d_state, sizeof(PcgState), cudaMemcpyDeviceToHost, op.stream), "state");
-        ICC_CUDA(cudaMemcpyAsync(ms.h_err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
-        ICC_CUDA(cudaStreamSynchronize(op.stream), "inner sync");
-        if (*ms.h_err) return timeout_error(*ms.h_err);   // a bounded wait ran out in this batch
-        const PcgState hs = *ms.h_state;
-        // the device state asks for a residual replacement when the FP32 recurrence has gained
-        // delta or after a bounded segment (an FP32 recurrence stalls once its drift from the true
-        // residual reaches the gain it is asked for), or stops on convergence, breakdown or NaN
-        if (hs.status == 0) {
-            if (launched > max_iter + 2 * int64_t(check_every))
+        ICC_CUDA(cudaMemcpyAsync(bt.h_state, bt.d_state, m * sizeof(PcgState), cudaMemcpyDeviceToHost, s), "state");
+        ICC_CUDA(cudaMemcpyAsync(bt.h_err, bt.d_err, sizeof(int), cudaMemcpyDeviceToHost, s), "err");
+        ICC_CUDA(cudaStreamSynchronize(s), "inner sync");
+        if (*bt.h_err) return timeout_error(*bt.h_err);   // a bounded wait ran out in this batch
+        // systems that asked for a replacement or stopped: reliable update x += sigma xs, r = b - A x in FP64
+        std::vector<size_t> upd;
+        for (size_t i = 0; i < m; ++i)
+            if (!items[i].done && bt.h_state[i].status != 0) upd.push_back(i);
+        if (upd.empty()) {
+            if (launched > max_budget + 2 * int64_t(check_every))
                 return set_error(ICC_TIMEOUT, "mixed solve: device state did not reach a stop condition");
             continue;
         }
-        // reliable update: x += sigma xs; r = b - A x in FP64
-        ru_accumulate_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_x64, ms.d_x32, sigma);
-        op.enqueue_apply(ms.d_x64, ms.d_y64, nullptr, nullptr);
-        ir_residual_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, b, ms.d_y64, ms.d_r64, op.d_partials);
-        sum_partials_kernel<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_scalars, 0);
-        launches += 5;
-        ICC_CUDA(cudaMemcpyAsync(ms.h_scalars, ms.d_scalars, 8, cudaMemcpyDeviceToHost, op.stream), "scalars");
-        ICC_CUDA(cudaStreamSynchronize(op.stream), "update sync");
-        updates++;
-        res = std::sqrt(ms.h_scalars[0]) / nb;
-        if (res < tol) {
-            status = ICC_OK;
-            break;
+        for (size_t i : upd) {
+            MixedItem &it = items[i];
+            Op &op = *it.op;
+            VecSet &v = *it.v;
+            ru_accumulate_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.x64, v.x32, it.nb);
+            op.enqueue_apply_on(s, v.x64, v.y64);
+            ir_residual_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, it.b, v.y64, v.r64, op.d_partials);
+            sum_partials_kernel<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_scalars, (int)i);
+            launches += 5;
         }
-        if (!std::isfinite(res) || hs.status == kStatNan) {
-            status = set_error(ICC_NAN, "mixed solve: non-finite residual (FP64 " + std::to_string(res) +
-                                            ", FP32 " + std::to_string(hs.rel_res) + ", p'Ap " +
-                                            std::to_string(hs.p_ap) + ", iteration " + std::to_string(hs.iter) +
-                                            ", update " + std::to_string(updates) + ")");
-            break;
+        ICC_CUDA(cudaMemcpyAsync(bt.h_scalars, bt.d_scalars, m * sizeof(double), cudaMemcpyDeviceToHost, s), "scalars");
+        ICC_CUDA(cudaStreamSynchronize(s), "update sync");
+        for (size_t i : upd) {
+            MixedItem &it = items[i];
+            Op &op = *it.op;
+            VecSet &v = *it.v;
+            const PcgState &hs = bt.h_state[i];
+            it.updates++;
+            it.iters = hs.iter;
+            it.res = std::sqrt(bt.h_scalars[i]) / it.nb;
+            bool stop = true;
+            if (it.res < it.tol) {
+                it.status = ICC_OK;
+            } else if (!std::isfinite(it.res) || hs.status == kStatNan) {
+                it.status = set_error(ICC_NAN, "mixed solve: non-finite residual (FP64 " + std::to_string(it.res) +
+                                                   ", FP32 " + std::to_string(hs.rel_res) + ", p'Ap " +
+                                                   std::to_string(hs.p_ap) + ", iteration " + std::to_string(hs.iter) +
+                                                   ", update " + std::to_string(it.updates) + ")");
+            } else if (hs.status == kStatBreakdown) {
+                it.status = ICC_BREAKDOWN;
+            } else if (hs.status == kStatMaxIter || hs.iter >= it.max_iter || it.updates >= max_updates) {
+                it.status = ICC_NOT_CONVERGED;
+            } else {
+                if (it.res < 0.9 * it.best) {
+                    it.best = it.res;
+                    it.no_progress = 0;
+                    stop = false;
+                } else {
+                    stop = ++it.no_progress >= max_no_progress;   // no longer reduces the true residual
+                }
+                it.status = ICC_NOT_CONVERGED;
+            }
+            if (stop) {
+                it.done = true;   // its state keeps a non-zero status, so the kernels skip it
+                active--;
+                continue;
+            }
+            ru_replace_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.r64, 1.0 / it.nb, v.inv32, v.r32,
+                                                                    op.d_partials);
+            ru_replace_finalize<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_state + i);
+            ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, it.res, delta, kMaxSegment, check_every);
+            // the direction update of this iteration, with the replaced residual
+            const bool ident = op.mask_mode == ICC_MASK_IDENTITY;
+            pcg_p_kernel<float><<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.r32, v.inv32, v.p32, bt.d_state + i,
+                                                                      op.mask_mode != ICC_MASK_NONE ? op.d_mask : nullptr,
+                                                                      ident ? v.xm32 : nullptr);
+            launches += 4;
         }
-        if (hs.status == kStatBreakdown) {
-            status = ICC_BREAKDOWN;
-            break;
-        }
-        if (hs.status == kStatMaxIter || hs.iter >= max_iter || updates >= max_updates) break;
-        if (res < 0.9 * best) {
-            best = res;
-            no_progress = 0;
-        } else if (++no_progress >= max_no_progress) {
-            break;  // FP32 recurrence no longer reduces the true residual: NOT_CONVERGED
-        }
-        ru_replace_kernel<<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r64, 1.0 / sigma, ms.d_inv32, ms.d_r32,
-                                                             op.d_partials);
-        ru_replace_finalize<<<1, kVecThreads, 0, op.stream>>>(op.d_partials, vb, ms.d_state);
-        ru_arm_kernel<<<1, 1, 0, op.stream>>>(ms.d_state, res, delta, kMaxSegment, check_every);
-        // the direction update of this iteration, with the replaced residual
-        const bool ident = op.mask_mode == ICC_MASK_IDENTITY;
-        pcg_p_kernel<float><<<vb, kVecThreads, 0, op.stream>>>(n, ms.d_r32, ms.d_inv32, ms.d_p32, ms.d_state,
-                                                               op.mask_mode != ICC_MASK_NONE ? op.d_mask : nullptr,
-                                                               ident ? ms.d_xm32 : nullptr);
-        launches += 4;
+        ICC_CUDA(cudaGetLastError(), "replacement");
     }
-    int err = 0;
-    ICC_CUDA(cudaMemcpyAsync(&err, ms.d_err, sizeof(int), cudaMemcpyDeviceToHost, op.stream), "err");
-    ICC_CUDA(cudaStreamSynchronize(op.stream), "err");
-    if (err) return timeout_error(err);
-    ICC_CUDA(cudaMemcpyAsync(x_out, ms.d_x64, (size_t)n * 8, cudaMemcpyDeviceToDevice, op.stream), "copy x");
-    *iters = ms.h_state->iter;
-    *rel_res = res;
-    op.last_info.iterations = ms.h_state->iter;
-    op.last_info.outer_iterations = updates;
-    op.last_info.rel_res = res;
-    op.last_info.fp64_applies = updates;
-    op.last_info.mixed_applies = ms.h_state->iter;
+    for (size_t i = 0; i < m; ++i) {
+        MixedItem &it = items[i];
+        it.rel_res = it.res;
+        ICC_CUDA(cudaMemcpyAsync(it.x_out, it.v->x64, (size_t)it.op->ndof * 8, cudaMemcpyDeviceToDevice, s), "copy x");
+    }
+    ICC_CUDA(cudaMemcpyAsync(bt.h_state, bt.d_state, m * sizeof(PcgState), cudaMemcpyDeviceToHost, s), "state");
+    ICC_CUDA(cudaStreamSynchronize(s), "mixed final");
+    for (size_t i = 0; i < m; ++i) items[i].iters = bt.h_state[i].iter;
+    if (launches_out) *launches_out = launches;
+    return ICC_OK;
+}
+
+// Captures the iteration graph of a batch: check_every x (persistent apply, fused vector step).
+static int capture_graph(MixedBatch &bt, int check_every) {
+    if (bt.graph) cudaGraphExecDestroy(bt.graph);
+    bt.graph = nullptr;
+    cudaGraph_t graph;
+    ICC_CUDA(cudaStreamBeginCapture(bt.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t ce = cudaSuccess;
+    for (int i = 0; i < check_every && ce == cudaSuccess; ++i) {
+        launch_apply_tc(bt.stream, bt.d_inst, bt.ninst, bt.nbricks, bt.bmat, bt.d_err, bt.num_sms);
+        ce = launch_tail(bt.stream, bt.d_inst, bt.ninst, bt.tail_grid, bt.d_ctr, bt.d_err, bt.limit);
+    }
+    cudaError_t ee = cudaStreamEndCapture(bt.stream, &graph);
+    ICC_CUDA(ce, "capture fused vector step");
+    ICC_CUDA(ee, "end capture");
+    cudaError_t e = cudaGraphInstantiate(&bt.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    ICC_CUDA(e, "graph instantiate");
+    return ICC_OK;
+}
+
+// One system: the handle's own vectors, state and cached graph.
+int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t max_iter, const icc_solve_opts &opts,
+                double *x_out, int64_t *iters, double *rel_res) {
+    int rc = op.ensure_pcg_buffers();
+    if (rc) return rc;
+    if ((rc = mixed_init(op))) return rc;
+    MixedState &ms = *op.mixed;
+    const int check_every = opts.check_every > 0 ? opts.check_every : 32;
+    std::vector<MixedItem> items(1);
+    items[0].op = &op;
+    items[0].v = &ms.v;
+    items[0].b = b;
+    items[0].diag = diag;
+    items[0].tol = tol;
+    items[0].max_iter = max_iter;
+    items[0].x_out = x_out;
+    MixedBatch bt;
+    bt.stream = op.stream;
+    bt.d_inst = ms.d_inst + 1;
+    bt.d_state = ms.d_state;
+    bt.h_state = ms.h_state;
+    bt.d_scalars = ms.d_scalars;
+    bt.h_scalars = ms.h_scalars;
+    bt.d_err = ms.d_err;
+    bt.h_err = ms.h_err;
+    bt.d_ctr = ms.d_grid_ctr;
+    bt.ninst = 1;
+    bt.nbricks = op.g.nbricks;
+    bt.tail_grid = share_ctas(items, tail_capacity(op))[0];
+    bt.num_sms = op.num_sms;
+    bt.bmat = ms.d_bmat;
+    bt.limit = ms.grid_wait_limit;
+    bt.graph = ms.graph;
+    if (!ms.graph || ms.graph_batch != check_every || ms.graph_limit != ms.grid_wait_limit) {
+        const TcInst I = make_inst(op, ms.v, ms.d_state, nullptr, 0, 0, bt.tail_grid, 1.f);
+        ICC_CUDA(cudaMemcpyAsync(bt.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
+        bt.graph = ms.graph;
+        if ((rc = capture_graph(bt, check_every))) return rc;
+        ms.graph = bt.graph;
+        ms.graph_batch = check_every;
+        ms.graph_limit = ms.grid_wait_limit;
+    }
+    int64_t launches = 0;
+    rc = run_mixed(bt, items, opts, &launches);
+    bt.graph = nullptr;   // stays with the handle
+    if (rc) return rc;
+    *iters = items[0].iters;
+    *rel_res = items[0].rel_res;
+    op.last_info.iterations = items[0].iters;
+    op.last_info.outer_iterations = items[0].updates;
+    op.last_info.rel_res = items[0].rel_res;
+    op.last_info.fp64_applies = items[0].updates;
+    op.last_info.mixed_applies = items[0].iters;
     op.last_info.kernel_launches = launches;
-    return status;
+    return items[0].status;
+}
+
+// Several systems at once: systems m of the call are (ops[m], vsets[m]) with right-hand side b[m]
+// (device), Jacobi diagonal diag[m] (device, null: the operator's own), tolerance tol[m] and
+// budget max_iter[m]; solutions into x[m] (device).  All operators must be on one device and have
+// element matrices of one shape (their uniform element matrices proportional).  The iterations of
+// all systems run in one persistent apply and one fused vector step per iteration, captured in
+// one CUDA graph; status[m], iters[m], rel_res[m], replacements[m] per system.  stream: where the
+// batch runs (every handle's own work is finished first).
+int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const std::vector<VecSet *> &vsets,
+                      const double *const *b, const double *const *diag, const double *tol, const int64_t *max_iter,
+                      const icc_solve_opts &opts, double *const *x, int *status, int64_t *iters, double *rel_res,
+                      int64_t *replacements) {
+    const size_t m = ops.size();
+    if (m == 0) return ICC_OK;
+    int rc;
+    for (Op *op : ops) {
+        if ((rc = op->ensure_pcg_buffers())) return rc;
+        if ((rc = mixed_init(*op))) return rc;
+        ICC_CUDA(cudaStreamSynchronize(op->stream), "batch: drain handle");
+    }
+    // every system's K_u must be the first one's times a factor (elements of one shape)
+    const std::vector<double> &K0 = ops[0]->mixed->kunif;
+    double k0max = 0.0;
+    for (double v : K0) k0max = std::fmax(k0max, std::fabs(v));
+    std::vector<float> kfac(m, 1.f);
+    for (size_t i = 0; i < m; ++i) {
+        const std::vector<double> &Ki = ops[i]->mixed->kunif;
+        double num = 0.0, den = 0.0;
+        for (size_t k = 0; k < Ki.size(); ++k) {
+            num += Ki[k] * K0[k];
+            den += K0[k] * K0[k];
+        }
+        const double f = num / den;
+        double dev = 0.0;
+        for (size_t k = 0; k < Ki.size(); ++k) dev = std::fmax(dev, std::fabs(Ki[k] - f * K0[k]));
+        if (!(dev <= 1e-9 * std::fabs(f) * k0max))
+            return set_error(ICC_BAD_ARG, "batched mixed solve: the systems' elements differ in shape (system " +
+                                              std::to_string(i) + ")");
+        kfac[i] = float(f);
+    }
+    std::vector<MixedItem> items(m);
+    int nbricks = 0;
+    std::vector<int> brick0(m);
+    for (size_t i = 0; i < m; ++i) {
+        items[i].op = ops[i];
+        items[i].v = vsets[i];
+        items[i].b = b[i];
+        items[i].diag = diag ? diag[i] : nullptr;
+        items[i].tol = tol[i];
+        items[i].max_iter = max_iter[i];
+        items[i].x_out = x[i];
+        items[i].kfac = kfac[i];
+        brick0[i] = nbricks;
+        nbricks += ops[i]->g.nbricks;
+    }
+    const int cap = tail_capacity(*ops[0]);
+    if ((int)m > cap) return set_error(ICC_BAD_ARG, "batched mixed solve: more systems than resident CTAs of the vector step");
+    const std::vector<int> ncta = share_ctas(items, cap);
+    MixedBatch bt;
+    bt.owned = true;
+    bt.stream = stream;
+    bt.ninst = (int)m;
+    bt.nbricks = nbricks;
+    bt.num_sms = ops[0]->num_sms;
+    bt.bmat = ops[0]->mixed->d_bmat;
+    bt.limit = ops[0]->mixed->grid_wait_limit;
+    if ((rc = dalloc(&bt.d_inst, m, "alloc batch")) || (rc = dalloc(&bt.d_state, m, "alloc batch")) ||
+        (rc = dalloc(&bt.d_scalars, m, "alloc batch")) || (rc = dalloc(&bt.d_err, 1, "alloc batch")) ||
+        (rc = dalloc(&bt.d_ctr, 1, "alloc batch")))
+        return rc;
+    ICC_CUDA(cudaMallocHost((void **)&bt.h_state, m * sizeof(PcgState)), "alloc pinned");
+    ICC_CUDA(cudaMallocHost((void **)&bt.h_scalars, m * sizeof(double)), "alloc pinned");
+    ICC_CUDA(cudaMallocHost((void **)&bt.h_err, sizeof(int)), "alloc pinned");
+    std::vector<TcInst> tab(m);
+    int cta = 0;
+    for (size_t i = 0; i < m; ++i) {
+        if (vsets[i]->part_cap < ncta[i]) return set_error(ICC_BAD_ARG, "batched mixed solve: partial buffer too small");
+        tab[i] = make_inst(*ops[i], *vsets[i], bt.d_state + i, nullptr, brick0[i], cta, ncta[i], kfac[i]);
+        cta += ncta[i];
+    }
+    bt.tail_grid = cta;
+    ICC_CUDA(cudaMemcpyAsync(bt.d_inst, tab.data(), m * sizeof(TcInst), cudaMemcpyHostToDevice, stream), "instance table");
+    const int check_every = opts.check_every > 0 ? opts.check_every : 32;
+    if ((rc = capture_graph(bt, check_every))) return rc;
+    rc = run_mixed(bt, items, opts, nullptr);
+    if (rc) return rc;
+    for (size_t i = 0; i < m; ++i) {
+        if (status) status[i] = items[i].status;
+        if (iters) iters[i] = items[i].iters;
+        if (rel_res) rel_res[i] = items[i].rel_res;
+        if (replacements) replacements[i] = items[i].updates;
+    }
+    return ICC_OK;
+}
+
+// Extra vector sets for systems that share a handle's operator (load cases).
+VecSet *mixed_vecset_create(Op &op) {
+    if (mixed_init(op)) return nullptr;
+    VecSet *v = new VecSet();
+    if (vecset_alloc(op, *v, tail_capacity(op))) {
+        vecset_free(*v);
+        delete v;
+        return nullptr;
+    }
+    return v;
+}
+
+void mixed_vecset_destroy(VecSet *v) {
+    if (!v) return;
+    vecset_free(*v);
+    delete v;
+}
+
+VecSet *mixed_own_vecset(Op &op) {
+    if (mixed_init(op)) return nullptr;
+    return &op.mixed->v;
 }
 
 }  // namespace icc

@@ -484,6 +484,18 @@ void Op::enqueue_apply(const double *x, double *y, double *partials, const PcgSt
                                                                   partials, st);
 }
 
+void Op::enqueue_apply_on(cudaStream_t s, const double *x, double *y) {
+    apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, s>>>(
+        g, x, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
+        nullptr);
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, s>>>(g, d_patch, nullptr, x, d_mask, mask_mode, extra64(), y,
+                                                             nullptr, nullptr);
+}
+
+void Op::enqueue_diagonal(double *d, cudaStream_t s) {
+    diagonal_kernel<<<vec_blocks, kVecThreads, 0, s>>>(g, d_scale, d_type_id, d_kdiag, sp_nnz ? d_sp_diag : nullptr, d);
+}
+
 int Op::apply_dev(const double *x, double *y) {
     enqueue_apply(x, y, nullptr, nullptr);
     ICC_CUDA(cudaGetLastError(), "apply launch");
@@ -767,9 +779,51 @@ int icc_pcg_solve_batched(int32_t count, icc_op *const *ops, const double *const
         if (std::adjacent_find(seen.begin(), seen.end()) != seen.end())
             return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: a handle appears twice (each instance needs its own)");
     }
-    // instances on worker threads, each solving on its handle's own stream: the GPU interleaves the
-    // instances' kernels (small grids leave SMs to the others); every solve is deterministic, so the
-    // results equal those of sequential calls
+    if (opts && opts->precision == ICC_MIXED && count > 0) {
+        // one batched solve: every iteration of all instances in one persistent tensor-core apply
+        // and one fused vector step, captured in one CUDA graph
+        std::vector<icc::Op *> o((size_t)count);
+        std::vector<icc::VecSet *> vs((size_t)count);
+        std::vector<const double *> bd((size_t)count), dd((size_t)count);
+        std::vector<double *> xd((size_t)count);
+        std::vector<double> tl((size_t)count, tol);
+        std::vector<int64_t> mi((size_t)count, max_iter), reps((size_t)count, 0);
+        const int dev = ops[0]->op.device;
+        for (int32_t i = 0; i < count; ++i) {
+            icc::Op &oi = ops[i]->op;
+            if (oi.device != dev) return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: handles on different devices");
+            if (max_iter < 0 || !(tol >= 0.0)) return set_error(ICC_BAD_ARG, "icc_pcg_solve_batched: bad tol or max_iter");
+            cudaSetDevice(oi.device);
+            int rc = oi.ensure_pcg_buffers();
+            if (rc) return rc;
+            o[(size_t)i] = &oi;
+            if (!(vs[(size_t)i] = icc::mixed_own_vecset(oi))) return ICC_BAD_ARG;
+            ICC_CUDA(cudaMemcpyAsync(oi.d_b, b[i], (size_t)oi.ndof * 8, cudaMemcpyHostToDevice, oi.stream), "batch h2d");
+            if (diag && diag[i])
+                ICC_CUDA(cudaMemcpyAsync(oi.d_diag, diag[i], (size_t)oi.ndof * 8, cudaMemcpyHostToDevice, oi.stream),
+                         "batch h2d");
+            bd[(size_t)i] = oi.d_b;
+            dd[(size_t)i] = (diag && diag[i]) ? oi.d_diag : nullptr;
+            xd[(size_t)i] = oi.d_y_out;
+        }
+        cudaStream_t s = ops[0]->op.stream;
+        std::vector<int> st((size_t)count, 0);
+        int rc = icc::mixed_solve_batch(s, o, vs, bd.data(), dd.data(), tl.data(), mi.data(), *opts, xd.data(), st.data(),
+                                        iters, rel_res, reps.data());
+        if (rc) return rc;
+        for (int32_t i = 0; i < count; ++i) {
+            ICC_CUDA(cudaMemcpyAsync(x[i], o[(size_t)i]->d_y_out, (size_t)o[(size_t)i]->ndof * 8, cudaMemcpyDeviceToHost, s),
+                     "batch d2h");
+            status[i] = st[(size_t)i];
+        }
+        ICC_CUDA(cudaStreamSynchronize(s), "batch d2h");
+        for (int32_t i = 0; i < count; ++i)
+            if (status[i] < 0) return set_error(status[i], "instance " + std::to_string(i) + " failed");
+        return ICC_OK;
+    }
+    // FP64: instances on worker threads, each solving on its handle's own stream: the GPU
+    // interleaves the instances' kernels (small grids leave SMs to the others); every solve is
+    // deterministic, so the results equal those of sequential calls
     std::atomic<int32_t> next(0);
     std::vector<std::string> errs((size_t)count);
     auto work = [&]() {

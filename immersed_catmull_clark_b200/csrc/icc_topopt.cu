@@ -301,6 +301,61 @@ static int solve_state_dev(icc_op *h, StateScratch &s, const double *force, cons
     return rc;
 }
 
+// The state solves of several load cases on one operator at once (rust/src/topopt_iga.rs:137-162
+// per case): b_k = F_k - K u_k on the free DOFs and its rescaled tolerance, then one batched
+// mixed-precision solve of all cases (their iterations share one persistent apply and one fused
+// vector step), then u_k += du_k on the free DOFs.  force and u hold nload vectors of n; bk and duk
+// are scratch of the same size; vsets[k] are the cases' FP32 vector sets.  iters = the summed
+// iterations.
+static int solve_states_batched(icc_op *h, StateScratch &s, int nload, const double *force, double *u, double *bk,
+                                double *duk, const std::vector<VecSet *> &vsets, double pcg_tol,
+                                const icc_solve_opts *opts, int64_t *iters) {
+    Op &o = h->op;
+    int rc;
+    if ((rc = state_scratch(o, s))) return rc;
+    const long long n = o.ndof;
+    const int nb = s.nblocks;
+    const uint8_t *mask = o.mask_mode != ICC_MASK_NONE ? o.d_mask : nullptr;
+    std::vector<double> tol((size_t)nload);
+    for (int k = 0; k < nload; ++k) {
+        const double *fk = force + (size_t)k * n;
+        double *uk = u + (size_t)k * n;
+        o.enqueue_apply(uk, s.ku0, nullptr, nullptr);
+        state_rhs_kernel<<<nb, kTopoThreads, 0, o.stream>>>(n, fk, s.ku0, mask, bk + (size_t)k * n, s.part);
+        double nf2 = 0.0, rb2 = 0.0;
+        if ((rc = reduce_to_host(o, s, s.part, nb, 0, &nf2))) return rc;
+        if ((rc = reduce_to_host(o, s, s.part + nb, nb, 0, &rb2))) return rc;
+        const double nfree = std::sqrt(nf2), rb = std::sqrt(rb2);
+        tol[(size_t)k] = rb > 0.0 ? std::fmin(pcg_tol * nfree / rb, 0.5) : 1.0;
+    }
+    if ((rc = o.diagonal_dev(s.diag))) return rc;
+    clamp_diag_kernel<<<nb, kTopoThreads, 0, o.stream>>>(n, s.diag, 1e-12);
+    ICC_CUDA(cudaStreamSynchronize(o.stream), "state set-up");
+    std::vector<Op *> ops((size_t)nload, &o);
+    std::vector<const double *> bp((size_t)nload), dp((size_t)nload, s.diag);
+    std::vector<double *> xp((size_t)nload);
+    std::vector<int64_t> mi((size_t)nload, 20 * n), its((size_t)nload, 0), reps((size_t)nload, 0);
+    std::vector<double> res((size_t)nload, 0.0);
+    std::vector<int> st((size_t)nload, 0);
+    for (int k = 0; k < nload; ++k) {
+        bp[(size_t)k] = bk + (size_t)k * n;
+        xp[(size_t)k] = duk + (size_t)k * n;
+    }
+    rc = mixed_solve_batch(o.stream, ops, vsets, bp.data(), dp.data(), tol.data(), mi.data(), *opts, xp.data(),
+                           st.data(), its.data(), res.data(), reps.data());
+    if (rc) return rc;
+    int64_t sum = 0;
+    for (int k = 0; k < nload; ++k) {
+        if (st[(size_t)k] < 0) return set_error(st[(size_t)k], "load case " + std::to_string(k) + ": state solve failed");
+        sum += its[(size_t)k];
+        double *uk = u + (size_t)k * n;
+        state_update_kernel<<<nb, kTopoThreads, 0, o.stream>>>(n, uk, duk + (size_t)k * n, mask, uk);
+    }
+    ICC_CUDA(cudaGetLastError(), "state update");
+    if (iters) *iters = sum;
+    return ICC_OK;
+}
+
 // ee = u_e^T K_e u_e, or ee += it (several load cases)
 static int energies_dev(Op &o, StateScratch &s, const double *u, double *ee, bool accumulate = false) {
     int rc;
@@ -328,8 +383,14 @@ struct icc_topopt {
     int4 *d_off = nullptr;
     int nst = 0, nblocks = 0;
     int nload = 1;   // load cases: d_force and d_u hold nload vectors of n
+    // batched mixed-precision state solves of several load cases: their right-hand sides and
+    // corrections (nload vectors of n each) and FP32 vector sets (case 0: the operator's own)
+    double *d_bk = nullptr, *d_duk = nullptr;
+    std::vector<icc::VecSet *> vsets;
     ~icc_topopt() {
-        void *p[] = {d_force, d_u, d_un, d_x, d_xold, d_cand, d_scale, d_ee, d_dcraw, d_dc, d_part, d_w, d_off};
+        for (size_t k = 1; k < vsets.size(); ++k) icc::mixed_vecset_destroy(vsets[k]);
+        void *p[] = {d_force, d_u, d_un, d_x, d_xold, d_cand, d_scale, d_ee, d_dcraw, d_dc, d_part, d_w, d_off,
+                     d_bk, d_duk};
         for (void *q : p)
             if (q) cudaFree(q);
         if (op) icc_op_destroy(op);
@@ -482,6 +543,12 @@ int icc_topopt_set_loads(icc_topopt *t, int32_t nload, const double *forces) {
     t->d_force = f;
     t->d_u = u;
     t->nload = nload;
+    // batched-solve buffers are sized for the previous number of cases
+    for (size_t k = 1; k < t->vsets.size(); ++k) icc::mixed_vecset_destroy(t->vsets[k]);
+    t->vsets.clear();
+    cudaFree(t->d_bk);
+    cudaFree(t->d_duk);
+    t->d_bk = t->d_duk = nullptr;
     return ICC_OK;
 }
 
@@ -505,17 +572,37 @@ int icc_topopt_run(icc_topopt *t, int32_t max_iter, double *compliance, double *
         ICC_CUDA(cudaMemcpyAsync(t->d_xold, t->d_x, (size_t)ne * 8, cudaMemcpyDeviceToDevice, o.stream), "x_old");
         icc::simp_scale_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(ne, t->d_x, c.emin, c.penal, t->d_scale);
         if ((rc = o.set_scale_dev(t->d_scale))) return rc;
-        // every load case: warm-started state, compliance F'u and energies, summed over the cases
+        // every load case: warm-started state, compliance F'u and energies, summed over the cases;
+        // with mixed precision and several cases, all their state solves run as one batch
         int64_t it = 0;
         double comp = 0.0;
+        const bool batched = t->nload > 1 && c.precision == ICC_MIXED;
+        if (batched) {
+            if (t->vsets.empty()) {
+                t->vsets.push_back(icc::mixed_own_vecset(o));
+                for (int k = 1; k < t->nload; ++k) t->vsets.push_back(icc::mixed_vecset_create(o));
+                for (auto *v : t->vsets)
+                    if (!v) return icc::set_error(ICC_OUT_OF_MEMORY, "icc_topopt_run: load-case vectors");
+            }
+            if (!t->d_bk) {
+                if ((rc = icc::dalloc(&t->d_bk, (size_t)t->nload * n, "alloc loads")) ||
+                    (rc = icc::dalloc(&t->d_duk, (size_t)t->nload * n, "alloc loads")))
+                    return rc;
+            }
+            rc = icc::solve_states_batched(t->op, s, t->nload, t->d_force, t->d_u, t->d_bk, t->d_duk, t->vsets,
+                                           c.pcg_tol, &opts, &it);
+            if (rc < 0) return rc;
+        }
         for (int k = 0; k < t->nload; ++k) {
             double *fk = t->d_force + (size_t)k * n, *uk = t->d_u + (size_t)k * n;
-            int64_t itk = 0;
-            double res = 0.0;
-            rc = icc::solve_state_dev(t->op, s, fk, uk, c.pcg_tol, &opts, t->d_un, &itk, &res);
-            if (rc < 0) return rc;
-            it += itk;
-            ICC_CUDA(cudaMemcpyAsync(uk, t->d_un, (size_t)n * 8, cudaMemcpyDeviceToDevice, o.stream), "state copy");
+            if (!batched) {
+                int64_t itk = 0;
+                double res = 0.0;
+                rc = icc::solve_state_dev(t->op, s, fk, uk, c.pcg_tol, &opts, t->d_un, &itk, &res);
+                if (rc < 0) return rc;
+                it += itk;
+                ICC_CUDA(cudaMemcpyAsync(uk, t->d_un, (size_t)n * 8, cudaMemcpyDeviceToDevice, o.stream), "state copy");
+            }
             double ck = 0.0;
             icc::dot_kernel<<<nb, icc::kTopoThreads, 0, o.stream>>>(n, fk, uk, t->d_part);
             if ((rc = icc::reduce_to_host(o, s, t->d_part, nb, 0, &ck))) return rc;
