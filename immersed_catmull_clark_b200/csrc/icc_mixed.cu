@@ -126,7 +126,8 @@ struct MixedState {
 //     TMEM) into one of two TMEM accumulators;
 //   warps 12-23 (epilogue, same split): read their 32 accumulator columns with tcgen05.ld and
 //     release them, sum the element results per patch node with warp shuffles (x, y) and a
-//     shared buffer (z), then write the brick partials (the node-side pass applies E).
+//     shared buffer (z), transform the node partials of bricks at the grid's ends by E, and
+//     write the brick partials.
 // mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full, fin.
 // Every wait is bounded.  On time-out the waiting thread raises a shared abort flag; every other
 // wait then returns false at once.  The builders and the epilogue decide at a barrier that ORs
@@ -142,7 +143,7 @@ constexpr int kAloFl = kTcM * kTcK;    // A_lo slot (shared memory, canonical K-
 constexpr uint32_t kALbo = (kTcM / 8) * 128;  // bytes between K-adjacent core matrices of A_lo
 constexpr uint32_t kPtTmemCols = 512;
 constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
-constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * 3 * kPVol + 2 * kZFl) * 4;  // 202,272 B
+constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * 3 * kPVol + 2 * kZFl + 3 * kPVol) * 4;  // 206,592 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
 // Each test may sleep up to kWaitSleepNs; with kWaitLimit tests a wait gives up after at most
@@ -236,6 +237,40 @@ __device__ __forceinline__ void edge_in(float *P, const Edge &E, int o, int ext,
 }
 
 // s_e times the system's K_u factor for brick row r (element lx + 8 ly + 32 lz), 0 outside the grid
+// W <- E W on the boundary control points of direction D of a brick's node partials P (patch
+// layout, origin o along D, ext of them inside the grid); line t along D is handled by thread t.
+// E couples only control points of a common element, so the partials of one brick transform on
+// their own and the transformed partials of all bricks add up to E applied to the node sums.
+template <int D>
+__device__ __forceinline__ void edge_out(float *P, const Edge &E, int o, int ext, int t) {
+    constexpr int LA = D == 0 ? kPY : kPX;
+    constexpr int LB = D == 2 ? kPY : kPZ;
+    constexpr int stride = D == 0 ? 1 : (D == 1 ? kPX : kPX * kPY);
+    if (t >= 3 * LA * LB) return;
+    const int c = t / (LA * LB), w = t - c * (LA * LB), a1 = w % LA, a2 = w / LA;
+    const int base = D == 0 ? c * kPVol + (a2 * kPY + a1) * kPX
+                            : (D == 1 ? c * kPVol + a2 * (kPY * kPX) + a1 : c * kPVol + a2 * kPX + a1);
+    const int nb = E.nb[D];
+    float u[4], v[4];
+    int loc[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int l = a < nb ? E.id[D][a] - o : -1;
+        loc[a] = (l >= 0 && l < ext) ? l : -1;
+        u[a] = loc[a] >= 0 ? P[base + loc[a] * stride] : 0.f;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        float acc = 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc = fmaf(E.e[D][a][b], u[b], acc);
+        v[a] = acc;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+        if (loc[a] >= 0) P[base + loc[a] * stride] = v[a];
+}
+
 __device__ __forceinline__ float row_scale(const TcInst &I, const BrickBox &bb, int r) {
     const int lx = r % kBX, ly = (r / kBX) % kBY, lz = r / (kBX * kBY);
     if (lx < bb.ex_n && ly < bb.ey_n && lz < bb.ez_n)
@@ -254,6 +289,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
     float *sP = sAlo + 2 * kAloFl;        // [3][3 * kPVol] input patches
     float *sZb = sP + 3 * 3 * kPVol;      // [2][kZFl] per-layer node partials, by brick parity
+    float *sW = sZb + 2 * kZFl;           // [3 * kPVol] node partials of a boundary brick (E applied)
     __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
@@ -489,16 +525,49 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             if (tc::named_sync_or(2, kRoleThreads, !ok || s_abort != 0)) break;
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
             const TcInst &I = insts[cur.i];
-            float *ob = I.patch + (size_t)(cur.b - I.brick0) * 3 * kPVol + et;
+            const int local = cur.b - I.brick0;
+            const unsigned fl = I.bflags[local];   // the same for every epilogue thread
+            float *ob = I.patch + (size_t)local * 3 * kPVol + et;
+            float sums[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                if (et + k * kRoleThreads >= 3 * kPVol) break;
                 float sum = 0.f;
+                if (et + k * kRoleThreads < 3 * kPVol) {
 #pragma unroll
-                for (int az = 0; az < 3; ++az)
-                    if (zpz[k] - az >= 0 && zpz[k] - az < kBZ) sum += sZ[zb[k] - 2 * 3 * (kPY * kPX) * az];
-                ob[k * kRoleThreads] = sum;
+                    for (int az = 0; az < 3; ++az)
+                        if (zpz[k] - az >= 0 && zpz[k] - az < kBZ) sum += sZ[zb[k] - 2 * 3 * (kPY * kPX) * az];
+                }
+                sums[k] = sum;
             }
+            if (fl) {
+                // W <- E W on the boundary planes of this brick's partials, one direction after the
+                // other (sW is reused by the next boundary brick only after the next brick's barrier,
+                // which every thread reaches after its reads below)
+                const BrickBox bb = brick_box(I.g, local);
+                const Edge &E = *I.edge;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (et + k * kRoleThreads < 3 * kPVol) sW[et + k * kRoleThreads] = sums[k];
+                tc::named_sync(2, kRoleThreads);
+                if (fl & 1u) {
+                    edge_out<0>(sW, E, bb.x0, min(kPX, I.g.cx - bb.x0), et);
+                    tc::named_sync(2, kRoleThreads);
+                }
+                if (fl & 2u) {
+                    edge_out<1>(sW, E, bb.y0, min(kPY, I.g.cy - bb.y0), et);
+                    tc::named_sync(2, kRoleThreads);
+                }
+                if (fl & 4u) {
+                    edge_out<2>(sW, E, bb.z0, min(kPZ, I.g.cz - bb.z0), et);
+                    tc::named_sync(2, kRoleThreads);
+                }
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    if (et + k * kRoleThreads < 3 * kPVol) sums[k] = sW[et + k * kRoleThreads];
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if (et + k * kRoleThreads < 3 * kPVol) ob[k * kRoleThreads] = sums[k];
         }
     } else if (lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
@@ -667,8 +736,7 @@ __device__ __forceinline__ void block_sum5(double (&v)[5]) {
 // One launch for everything of a PCG iteration after the operator (rust/src/solver.rs:38-71),
 // with one grid-wide barrier, for every system of the batch: system i is served by CTAs
 // [cta0, cta0 + ncta) and reduces its own partials.
-//   Phase A, node by node: Ap = the node sum of the brick partials (with the boundary extraction)
-//   plus the sparse term, output rule applied; and five dot products p'Ap, z'Ap, Ap'D^-1 Ap, r'Ap,
+//   Phase A, node by node: Ap = the node sum of the brick partials plus the sparse term, output rule applied; and five dot products p'Ap, z'Ap, Ap'D^-1 Ap, r'Ap,
 //   Ap'Ap (z = D^-1 r).
 //   Barrier.  Every CTA of the system reduces the same partials in the same order: alpha =
 //   r'z / p'Ap, and for r_new = r - alpha Ap, without another reduction,
@@ -682,7 +750,7 @@ __device__ __forceinline__ void block_sum5(double (&v)[5]) {
 //   the formulas (so they bridge one iteration only).
 // The system's first CTA writes its state.  All CTAs of a system take the same branches; the CTAs
 // of a stopped system only arrive at the barrier.
-__global__ void __launch_bounds__(kTailThreads)
+__global__ void __launch_bounds__(kTailThreads, 4)
 pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long *ctr, int *err, long long wait_limit) {
     __shared__ PcgState S;
     __shared__ double s_ab[2];
@@ -728,17 +796,13 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
     const long long n = 3 * g.nsc;
     // A. Ap at every node and the five dot products
     double dA[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const Edge *E = I.edge && (I.edge->nb[0] | I.edge->nb[1] | I.edge->nb[2]) ? I.edge : nullptr;
     // 32-bit index arithmetic: the set-up checks nsc < 2^31
     const unsigned ucx = (unsigned)g.cx, ucy = (unsigned)g.cy;
     for (long long nd = t0; nd < g.nsc; nd += T) {
         const unsigned u = (unsigned)nd, q1 = u / ucx;
         const int ix = int(u - q1 * ucx), iy = int(q1 % ucy), iz = int(q1 / ucy);
         float sv[3];
-        const int sx = E ? edge_slot(*E, 0, ix) : -1, sy = E ? edge_slot(*E, 1, iy) : -1,
-                  sz = E ? edge_slot(*E, 2, iz) : -1;
-        if (sx < 0 && sy < 0 && sz < 0) node_partials(g, I.patch, ix, iy, iz, sv[0], sv[1], sv[2]);
-        else edge_node(g, *E, I.patch, ix, iy, iz, sx, sy, sz, sv);
+        node_partials(g, I.patch, ix, iy, iz, sv[0], sv[1], sv[2]);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const long long idx = (long long)c * g.nsc + nd;
@@ -1225,7 +1289,7 @@ static int enqueue_apply_tc(Op &op, const float *x, float *y) {
     const TcInst I = make_inst(op, ms.v, nullptr, xin, 0, 0, 0, 1.f);
     ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
     launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_bmat, ms.d_err, op.num_sms);
-    gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, ms.d_edge, x, op.d_mask,
+    gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
                                                                        op.mask_mode, op.extra32(), y, nullptr, nullptr);
     ICC_CUDA(cudaGetLastError(), "tc apply launch");
     return ICC_OK;
@@ -1287,7 +1351,7 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
         cudaEventRecord(ev[3 * r], op.stream);
         launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_bmat, ms.d_err, op.num_sms);
         cudaEventRecord(ev[3 * r + 1], op.stream);
-        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, ms.d_edge, x, op.d_mask,
+        gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
                                                                            ICC_MASK_NONE, op.extra32(), y, nullptr,
                                                                            nullptr);
         cudaEventRecord(ev[3 * r + 2], op.stream);

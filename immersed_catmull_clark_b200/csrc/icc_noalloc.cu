@@ -210,7 +210,7 @@ extern "C" int icc_apply_f64_noalloc(const int64_t nel_dir[3], const double *ke_
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     apply_f64_noalloc_kernel<<<g.nbricks, kApplyThreads, kApplySmem, s>>>(g, x_dev, scale_dev, ke_types_dev, ntypes,
                                                                          type_id_dev, scratch);
-    gather_kernel<double><<<sms * 4, kVecThreads, 0, s>>>(g, scratch, nullptr, x_dev, nullptr, ICC_MASK_NONE, Sparse<double>(), y_dev, nullptr,
+    gather_kernel<double><<<sms * 4, kVecThreads, 0, s>>>(g, scratch, x_dev, nullptr, ICC_MASK_NONE, Sparse<double>(), y_dev, nullptr,
                                                           nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "icc_apply_f64_noalloc: launch");

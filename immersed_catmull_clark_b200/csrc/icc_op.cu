@@ -480,7 +480,7 @@ void Op::enqueue_apply(const double *x, double *y, double *partials, const PcgSt
     apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
         g, x, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
         st);
-    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, nullptr, x, d_mask, mask_mode, extra64(), y,
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, x, d_mask, mask_mode, extra64(), y,
                                                                   partials, st);
 }
 
@@ -488,7 +488,7 @@ void Op::enqueue_apply_on(cudaStream_t s, const double *x, double *y) {
     apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, s>>>(
         g, x, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
         nullptr);
-    gather_kernel<double><<<vec_blocks, kVecThreads, 0, s>>>(g, d_patch, nullptr, x, d_mask, mask_mode, extra64(), y,
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, s>>>(g, d_patch, x, d_mask, mask_mode, extra64(), y,
                                                              nullptr, nullptr);
 }
 
@@ -531,7 +531,7 @@ void Op::enqueue_pcg_iteration() {
     apply_f64_kernel<<<g.nbricks, kApplyThreads, kApplySmem, stream>>>(
         g, d_p, d_mask, mask_mode != ICC_MASK_NONE, d_scale, d_kfrag, d_tile_start, d_tile_type, d_tile_elem, d_patch,
         d_state);
-    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, nullptr, d_p, d_mask, mask_mode, extra64(), d_ap,
+    gather_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(g, d_patch, d_p, d_mask, mask_mode, extra64(), d_ap,
                                                                   d_partials,
                                                                   d_state, d_state, d_counter);
     pcg_update_kernel<double><<<vec_blocks, kVecThreads, 0, stream>>>(ndof, d_p, d_ap, d_inv, d_x, d_r, d_partials,
@@ -866,7 +866,7 @@ int icc_op_profile_apply(icc_op *op, const double *x_dev, double *y_dev, int32_t
             o.d_tile_elem, o.d_patch, nullptr);
         cudaEventRecord(ev[3 * r + 1], o.stream);
         icc::gather_kernel<double><<<o.vec_blocks, icc::kVecThreads, 0, o.stream>>>(
-            o.g, o.d_patch, nullptr, x_dev, o.d_mask, o.mask_mode, o.extra64(), y_dev, nullptr, nullptr);
+            o.g, o.d_patch, x_dev, o.d_mask, o.mask_mode, o.extra64(), y_dev, nullptr, nullptr);
         cudaEventRecord(ev[3 * r + 2], o.stream);
     }
     cudaError_t e = cudaEventSynchronize(ev.back());

@@ -88,40 +88,6 @@ __device__ __forceinline__ void node_partials(const Geom &g, const T *__restrict
             }
 }
 
-// (E W) at a control point with boundary slots (sx, sy, sz) (-1: E is the identity along that
-// direction there), W = the node sums of the brick partials: the sum over the <= 4 x 4 x 4
-// coupled control points with the weights of E, in a fixed order.
-template <class T>
-__device__ __noinline__ void edge_node(const Geom &g, const Edge &E, const T *__restrict__ patch, int ix, int iy, int iz,
-                                       int sx, int sy, int sz, T out[3]) {
-    T a0 = T(0), a1 = T(0), a2 = T(0);
-    const int mx = sx < 0 ? 1 : E.nb[0], my = sy < 0 ? 1 : E.nb[1], mz = sz < 0 ? 1 : E.nb[2];
-    for (int cz = 0; cz < mz; ++cz) {
-        const float wz = sz < 0 ? 1.f : E.e[2][sz][cz];
-        if (wz == 0.f) continue;
-        const int jz = sz < 0 ? iz : E.id[2][cz];
-        for (int cy = 0; cy < my; ++cy) {
-            const float wy = sy < 0 ? 1.f : E.e[1][sy][cy];
-            if (wy == 0.f) continue;
-            const int jy = sy < 0 ? iy : E.id[1][cy];
-            for (int cx = 0; cx < mx; ++cx) {
-                const float wx = sx < 0 ? 1.f : E.e[0][sx][cx];
-                if (wx == 0.f) continue;
-                const int jx = sx < 0 ? ix : E.id[0][cx];
-                T s0, s1, s2;
-                node_partials(g, patch, jx, jy, jz, s0, s1, s2);
-                const T w = T(wz * wy * wx);
-                a0 += w * s0;
-                a1 += w * s1;
-                a2 += w * s2;
-            }
-        }
-    }
-    out[0] = a0;
-    out[1] = a1;
-    out[2] = a2;
-}
-
 // Row idx of the sparse term applied to the masked input: sum_k S[idx][k] (m .* p)[k].
 template <class T>
 __device__ __forceinline__ T sparse_row(const Sparse<T> &sp, long long idx, const T *__restrict__ p,
@@ -136,14 +102,14 @@ __device__ __forceinline__ T sparse_row(const Sparse<T> &sp, long long idx, cons
     return acc;
 }
 
-// y = sum of the brick partials of each node (fixed order; with `edge`, transformed by the
-// boundary extraction E) plus the sparse term, output mask applied; optionally the CTA partial of
-// p'y (in double), and with `fuse` the alpha step in the last CTA.
+// y = sum of the brick partials of each node (fixed order) plus the sparse term, output mask
+// applied; optionally the CTA partial of p'y (in double), and with `fuse` the alpha step in the
+// last CTA.
 template <class T>
 __global__ void __launch_bounds__(kVecThreads)
-gather_kernel(Geom g, const T *__restrict__ patch, const Edge *__restrict__ edge, const T *__restrict__ p,
-              const uint8_t *__restrict__ mask, int mask_mode, Sparse<T> sp, T *__restrict__ y,
-              double *__restrict__ partials, const PcgState *st, PcgState *fuse = nullptr, unsigned *counter = nullptr) {
+gather_kernel(Geom g, const T *__restrict__ patch, const T *__restrict__ p, const uint8_t *__restrict__ mask,
+              int mask_mode, Sparse<T> sp, T *__restrict__ y, double *__restrict__ partials, const PcgState *st,
+              PcgState *fuse = nullptr, unsigned *counter = nullptr) {
     if (st && st->status != 0) return;
     double dot = 0.0;
     // one warp per row (iy, iz) of control points, lanes along x: the brick partials of
@@ -156,30 +122,21 @@ gather_kernel(Geom g, const T *__restrict__ patch, const Edge *__restrict__ edge
         int by[2], ly[2], bz[2], lz[2];
         const int nby = node_bricks(iy, kBY, g.nby, by, ly);
         const int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
-        const int sy = edge ? edge_slot(*edge, 1, iy) : -1, sz = edge ? edge_slot(*edge, 2, iz) : -1;
         for (int ix = lane; ix < g.cx; ix += 32) {
             const long long n = (long long)row * g.cx + ix;
-            const int sx = edge ? edge_slot(*edge, 0, ix) : -1;
-            T sv[3];
-            if (sx < 0 && sy < 0 && sz < 0) {
-                int bx[2], lx[2];
-                const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
-                T s0 = T(0), s1 = T(0), s2 = T(0);
-                for (int a = 0; a < nbz; ++a)
-                    for (int q = 0; q < nby; ++q)
-                        for (int w = 0; w < nbx; ++w) {
-                            size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
-                            const T *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
-                            s0 += pb[0];
-                            s1 += pb[kPVol];
-                            s2 += pb[2 * kPVol];
-                        }
-                sv[0] = s0;
-                sv[1] = s1;
-                sv[2] = s2;
-            } else {
-                edge_node(g, *edge, patch, ix, iy, iz, sx, sy, sz, sv);
-            }
+            int bx[2], lx[2];
+            const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
+            T s0 = T(0), s1 = T(0), s2 = T(0);
+            for (int a = 0; a < nbz; ++a)
+                for (int q = 0; q < nby; ++q)
+                    for (int w = 0; w < nbx; ++w) {
+                        size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
+                        const T *pb = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
+                        s0 += pb[0];
+                        s1 += pb[kPVol];
+                        s2 += pb[2 * kPVol];
+                    }
+            T sv[3] = {s0, s1, s2};
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 long long idx = (long long)c * g.nsc + n;
