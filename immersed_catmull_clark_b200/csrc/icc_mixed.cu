@@ -54,18 +54,26 @@ __host__ __device__ __forceinline__ int canon(int row, int k, int rows) {
     return (k >> 2) * (rows / 8) * 32 + (row >> 3) * 32 + (row & 7) * 4 + (k & 3);
 }
 
+// One brick of a batch, precomputed on the host so the kernel needs no integer divisions: its
+// system, its index within the system, its brick coordinates and extent, and its boundary flags
+// (bit d: the brick's patch holds boundary control points of direction d).
+struct BrickDesc {
+    int inst, local;
+    unsigned xyz;   // bx | by << 11 | bz << 22
+    unsigned ext;   // ex_n | ey_n << 4 | ez_n << 8 | flags << 12
+};
+constexpr int kMaxListPerCta = 2048;   // bricks of one persistent CTA in one launch, at most
+
 // One system of a mixed solve as the kernels see it: the operator data of its handle and its own
 // FP32 vectors.  A solve of one system is a batch of one; a batch of several (designs of uneven
 // sizes, or load cases of one operator) runs every iteration as one persistent apply over all
 // bricks of all systems and one fused vector step whose CTAs are shared out among the systems.
 struct TcInst {
     Geom g;
-    int brick0;                  // first brick of the system in the batch's brick numbering
     int cta0, ncta;              // CTAs of the fused vector step that serve it
     float kfac;                  // the system's K_u = kfac * the batch's K_u (same element shape)
     const float *xin;            // input of the brick apply (p, or the masked copy pm)
     const float *scale;          // s_e (FP32)
-    const uint8_t *bflags;
     const Edge *edge;
     float *patch;                // brick partials [nbricks][3][kPVol]
     const uint8_t *mask;         // output rule of the fused vector step (null: none)
@@ -92,7 +100,8 @@ struct MixedState {
     std::vector<double> kunif;       // K_u (host), to compare systems of a batch
     Edge edge{};
     Edge *d_edge = nullptr;          // the same in device memory, for the node-side passes
-    uint8_t *d_bflags = nullptr;     // per brick: bit d set when its patch holds boundary points of d
+    std::vector<uint8_t> flags;      // per brick: bit d set when its patch holds boundary points of d
+    BrickDesc *d_desc = nullptr;     // the handle's bricks as system 0 of a batch
     float *d_scale32 = nullptr;
     double *d_scalars = nullptr, *h_scalars = nullptr;
     int *d_err = nullptr;
@@ -165,42 +174,19 @@ struct BrickBox {
     int x0, y0, z0, ex_n, ey_n, ez_n;
 };
 
-__device__ __forceinline__ BrickBox brick_box(const Geom &g, int local) {
-    const int bx = local % g.nbx, by = (local / g.nbx) % g.nby, bz = local / (g.nbx * g.nby);
+
+__device__ __forceinline__ BrickBox desc_box(const BrickDesc &d) {
     BrickBox r;
-    r.x0 = bx * kBX;
-    r.y0 = by * kBY;
-    r.z0 = bz * kBZ;
-    r.ex_n = min(kBX, g.nx - r.x0);
-    r.ey_n = min(kBY, g.ny - r.y0);
-    r.ez_n = min(kBZ, g.nz - r.z0);
+    r.x0 = int(d.xyz & 2047u) * kBX;
+    r.y0 = int((d.xyz >> 11) & 2047u) * kBY;
+    r.z0 = int(d.xyz >> 22) * kBZ;
+    r.ex_n = int(d.ext & 15u);
+    r.ey_n = int((d.ext >> 4) & 15u);
+    r.ez_n = int((d.ext >> 8) & 15u);
     return r;
 }
 
-// The bricks of a persistent CTA: blockIdx.x, blockIdx.x + gridDim.x, ... in the batch's brick
-// numbering, without the bricks of systems whose solve has stopped (their state does not change
-// while the kernel runs, so every role of the CTA walks the same sequence).
-struct BrickCursor {
-    int b, i;   // brick of the batch and its system; b >= nbricks when the walk is over
-    __device__ __forceinline__ void settle(const TcInst *__restrict__ I, int ninst, int nbricks) {
-        while (b < nbricks) {
-            while (i + 1 < ninst && b >= I[i + 1].brick0) ++i;
-            const PcgState *st = I[i].st;
-            if (!st || __ldcg(&st->status) == 0) return;
-            const int end = i + 1 < ninst ? I[i + 1].brick0 : nbricks;
-            b += ((end - b + (int)gridDim.x - 1) / (int)gridDim.x) * (int)gridDim.x;
-        }
-    }
-    __device__ __forceinline__ void start(const TcInst *__restrict__ I, int ninst, int nbricks) {
-        b = blockIdx.x;
-        i = 0;
-        settle(I, ninst, nbricks);
-    }
-    __device__ __forceinline__ void next(const TcInst *__restrict__ I, int ninst, int nbricks) {
-        b += gridDim.x;
-        settle(I, ninst, nbricks);
-    }
-};
+__device__ __forceinline__ unsigned desc_flags(const BrickDesc &d) { return (d.ext >> 12) & 7u; }
 
 // V = E' u on the boundary control points of direction D inside the patch P (3 x kPZ x kPY x kPX,
 // patch origin o along D, ext of its control points inside the grid); line t along D (t < the
@@ -282,8 +268,8 @@ __device__ __forceinline__ float row_scale(const TcInst &I, const BrickBox &bb, 
 // 25 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
 // the compiler caps a thread at 72
 __global__ void __launch_bounds__(kPtThreads, 1)
-apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const float4 *__restrict__ bmat,
-                int *__restrict__ err) {
+apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const BrickDesc *__restrict__ desc,
+                const float4 *__restrict__ bmat, int *__restrict__ err) {
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
     float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
@@ -293,15 +279,45 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
+    // this CTA's bricks of systems whose solve goes on: bricks blockIdx.x + k gridDim.x in order
+    __shared__ int s_list[kMaxListPerCta];
+    __shared__ int s_cnt[32];
+    __shared__ int s_nlist;
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
              *fin = bars + 9;
-    {
-        BrickCursor c0;
-        c0.start(insts, ninst, nbricks);
-        if (c0.b >= nbricks) return;   // nothing for this CTA (the same for all its threads)
-    }
-
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        // stream compaction, kPtThreads candidates per round: each warp ballots its 32, the counts
+        // give every warp its offset, the list keeps the order of the bricks
+        const int G = gridDim.x, L = (nbricks - (int)blockIdx.x + G - 1) / G;
+        constexpr int kW = kPtThreads / 32;
+        if (tid == 0) s_nlist = 0;
+        __syncthreads();
+        for (int base = 0; base < L; base += kPtThreads) {
+            const int k = base + tid;
+            bool a = false;
+            if (k < L) {
+                const PcgState *st = insts[desc[blockIdx.x + k * G].inst].st;
+                a = !st || __ldcg(&st->status) == 0;
+            }
+            const unsigned act = __ballot_sync(0xffffffffu, a);
+            if (lane == 0) s_cnt[warp] = __popc(act);
+            __syncthreads();
+            int off = s_nlist;
+            for (int w2 = 0; w2 < warp; ++w2) off += s_cnt[w2];
+            if (a) s_list[off + __popc(act & ((1u << lane) - 1u))] = blockIdx.x + k * G;
+            __syncthreads();
+            if (tid == 0) {
+                int t = s_nlist;
+                for (int w2 = 0; w2 < kW; ++w2) t += s_cnt[w2];
+                s_nlist = t;
+            }
+            __syncthreads();
+        }
+        if (s_nlist == 0) return;   // nothing for this CTA (the same for all its threads)
+    }
+    const int nmine = s_nlist;
+
     if (warp == 0) {
         tc::tmem_alloc(&tmem_base, kPtTmemCols);
         tc::tmem_relinquish();
@@ -334,11 +350,12 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         // patch rows (c, pz, py) of kPX floats; thread tid < 108 copies row tid, in 8-byte pieces
         // when the row is whole and starts on an even float (always when the x control-point
         // count is even), else float by float
-        auto load_patch = [&](const BrickCursor &cu, float *dst) {
-            if (cu.b < nbricks && tid < 3 * kPZ * kPY) {
-                const TcInst &I = insts[cu.i];
+        auto load_patch = [&](int k, float *dst) {
+            if (k < nmine && tid < 3 * kPZ * kPY) {
+                const BrickDesc d = desc[s_list[k]];
+                const TcInst &I = insts[d.inst];
                 const Geom &g = I.g;
-                const BrickBox bb = brick_box(g, cu.b - I.brick0);
+                const BrickBox bb = desc_box(d);
                 const int rc = tid / (kPZ * kPY), py = tid % kPY, pz = (tid / kPY) % kPZ;
                 const int gy = bb.y0 + py, gz = bb.z0 + pz;
                 float *drow = dst + tid * kPX;
@@ -363,32 +380,26 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             tc::cp_async_commit();
         };
         // three patch buffers: the brick two ahead is fetched while one is built
-        BrickCursor cur, ld;
-        cur.start(insts, ninst, nbricks);
-        ld = cur;
-        load_patch(ld, sP);
-        ld.next(insts, ninst, nbricks);
-        load_patch(ld, sP + 3 * kPVol);
-        ld.next(insts, ninst, nbricks);
+        load_patch(0, sP);
+        load_patch(1, sP + 3 * kPVol);
         const int r = q * 32 + lane;
-        unsigned fl_next = insts[cur.i].bflags[cur.b - insts[cur.i].brick0];
-        float se_next = row_scale(insts[cur.i], brick_box(insts[cur.i].g, cur.b - insts[cur.i].brick0), r);
-        for (int it = 0; cur.b < nbricks; ++it) {
+        BrickDesc dn = desc[s_list[0]];
+        unsigned fl_next = desc_flags(dn);
+        float se_next = row_scale(insts[dn.inst], desc_box(dn), r);
+        for (int it = 0; it < nmine; ++it) {
             const int s = it & 1, pb = it % 3;
             const unsigned fl = fl_next;   // bit d: the brick's patch holds boundary points of d
             const float se = se_next;      // s_e k of this thread's element (0 outside the grid)
-            const TcInst &I = insts[cur.i];
+            const BrickDesc d = dn;
+            const TcInst &I = insts[d.inst];
             const Geom &g = I.g;
-            const BrickBox bb = brick_box(g, cur.b - I.brick0);
-            BrickCursor nx = cur;
-            nx.next(insts, ninst, nbricks);
-            if (nx.b < nbricks) {
-                const TcInst &In = insts[nx.i];
-                fl_next = In.bflags[nx.b - In.brick0];
-                se_next = row_scale(In, brick_box(In.g, nx.b - In.brick0), r);
+            const BrickBox bb = desc_box(d);
+            if (it + 1 < nmine) {
+                dn = desc[s_list[it + 1]];
+                fl_next = desc_flags(dn);
+                se_next = row_scale(insts[dn.inst], desc_box(dn), r);
             }
-            load_patch(ld, sP + ((it + 2) % 3) * 3 * kPVol);
-            ld.next(insts, ninst, nbricks);
+            load_patch(it + 2, sP + ((it + 2) % 3) * 3 * kPVol);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const float vm = valid ? se : 0.f;
             tc::cp_async_wait<2>();
@@ -442,7 +453,6 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             tc::fence_before_sync();
             tc::mbar_arrive(&a_full[s]);
             tc::named_sync(1, kRoleThreads);   // everyone is done with this patch before it is refilled
-            cur = nx;
         }
         tc::cp_async_wait<0>();
     } else if (warp < 2 * kRoleWarps) {
@@ -469,11 +479,10 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             zb[k] = 9 * (kPY * kPX) * pz + (kPY * kPX) * ci + pyx;
             zpz[k] = pz;
         }
-        BrickCursor cur;
-        cur.start(insts, ninst, nbricks);
-        for (int it = 0; cur.b < nbricks; ++it, cur.next(insts, ninst, nbricks)) {
+        for (int it = 0; it < nmine; ++it) {
             float *sZ = sZb + (it & 1) * kZFl;
             const int db = it & 1;
+            const BrickDesc d = desc[s_list[it]];
             // on a failed wait the values read below are not used: the barrier before the z-sum
             // makes every epilogue thread leave the loop
             const bool ok = pt_wait(&d_full[db], uint32_t(it >> 1) & 1u, &s_abort, err);
@@ -524,9 +533,9 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             // the other buffer) finished before its thread reached this barrier
             if (tc::named_sync_or(2, kRoleThreads, !ok || s_abort != 0)) break;
             // z: node pz = lz + az; sum the <= 3 layers in increasing az
-            const TcInst &I = insts[cur.i];
-            const int local = cur.b - I.brick0;
-            const unsigned fl = I.bflags[local];   // the same for every epilogue thread
+            const TcInst &I = insts[d.inst];
+            const int local = d.local;
+            const unsigned fl = desc_flags(d);   // the same for every epilogue thread
             float *ob = I.patch + (size_t)local * 3 * kPVol + et;
             float sums[3];
 #pragma unroll
@@ -543,7 +552,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
                 // W <- E W on the boundary planes of this brick's partials, one direction after the
                 // other (sW is reused by the next boundary brick only after the next brick's barrier,
                 // which every thread reaches after its reads below)
-                const BrickBox bb = brick_box(I.g, local);
+                const BrickBox bb = desc_box(d);
                 const Edge &E = *I.edge;
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
@@ -580,11 +589,8 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         // so adding a step's offset never carries out of the address field
         const uint64_t dbh0 = tc::make_desc(sB, kBLbo, kSbo), dbl0 = tc::make_desc(sB + kBFl, kBLbo, kSbo);
         const uint64_t dal0 = tc::make_desc(sAlo, kALbo, kSbo), dal1 = tc::make_desc(sAlo + kAloFl, kALbo, kSbo);
-        BrickCursor cur;
-        cur.start(insts, ninst, nbricks);
-        int nmine = 0;   // bricks issued
-        for (; cur.b < nbricks && run; cur.next(insts, ninst, nbricks), ++nmine) {
-            const int it = nmine, s = it & 1, db = it & 1;
+        for (int it = 0; it < nmine && run; ++it) {
+            const int s = it & 1, db = it & 1;
             // slot s holds brick it, and brick it - 2 has been drained from accumulator buffer db;
             // on a failed wait nothing more is issued
             run = pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err) &&
@@ -648,10 +654,10 @@ ir_init_kernel(long long n, const double *__restrict__ b, double *__restrict__ x
     if (threadIdx.x == 0) partials[blockIdx.x] = bb;
 }
 
-// r32 = r / |r| (FP32), |r|^2 in scalars[0]
+// r32 = r / |r| (FP32), |r|^2 in scalars[0] (r = 0 gives r32 = 0)
 __global__ void ir_to_f32_kernel(long long n, const double *__restrict__ r, float *__restrict__ r32,
                                  const double *__restrict__ scalars) {
-    const double inv = 1.0 / sqrt(scalars[0]);
+    const double inv = scalars[0] > 0.0 ? 1.0 / sqrt(scalars[0]) : 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         r32[i] = float(r[i] * inv);
 }
@@ -1125,9 +1131,28 @@ static void vecset_free(VecSet &v) {
 // CTAs of the fused vector step that can be resident at once (its grid barrier needs all of them)
 static int tail_capacity(const Op &op) { return op.mixed->tail_per_sm * op.num_sms; }
 
+// The bricks of system `inst` (the handle op) in brick order, for a batch's brick list.
+static void append_descs(const Op &op, int inst, std::vector<BrickDesc> &out) {
+    const Geom &g = op.g;
+    const std::vector<uint8_t> &fl = op.mixed->flags;
+    for (int b = 0; b < g.nbricks; ++b) {
+        const int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
+        BrickDesc d;
+        d.inst = inst;
+        d.local = b;
+        d.xyz = unsigned(bx) | unsigned(by) << 11 | unsigned(bz) << 22;
+        const unsigned ex = unsigned(std::min(kBX, g.nx - bx * kBX)), ey = unsigned(std::min(kBY, g.ny - by * kBY)),
+                       ez = unsigned(std::min(kBZ, g.nz - bz * kBZ));
+        d.ext = ex | ey << 4 | ez << 8 | unsigned(fl[(size_t)b]) << 12;
+        out.push_back(d);
+    }
+}
+
 static int mixed_init(Op &op) {
     if (op.mixed && op.mixed->ready) return ICC_OK;
     if (op.g.nsc >= (1LL << 31)) return set_error(ICC_BAD_ARG, "tensor-core path: more than 2^31 control points");
+    if (op.g.nbx > 2047 || op.g.nby > 2047 || op.g.nbz > 2047)
+        return set_error(ICC_BAD_ARG, "tensor-core path: more than 2047 bricks along a direction");
     if (!op.mixed) op.mixed = new MixedState();
     MixedState &ms = *op.mixed;
     int rc = setup_edge(op, ms.edge, ms.kunif);
@@ -1163,11 +1188,17 @@ static int mixed_init(Op &op) {
                     if (ms.edge.id[d][a] >= o && ms.edge.id[d][a] < o + ext) fl[(size_t)b] |= uint8_t(1u << d);
             }
         }
-        if ((rc = dalloc(&ms.d_bflags, fl.size(), "alloc brick flags"))) return rc;
+        ms.flags = fl;
+        if ((g.nbricks + op.num_sms - 1) / op.num_sms > kMaxListPerCta)
+            return set_error(ICC_BAD_ARG, "tensor-core path: more than 2048 bricks per SM");
+        std::vector<BrickDesc> dv;
+        append_descs(op, 0, dv);
+        if ((rc = dalloc(&ms.d_desc, dv.size(), "alloc brick list"))) return rc;
         if ((rc = dalloc(&ms.d_edge, 1, "alloc edge"))) return rc;
-        ICC_CUDA(cudaMemcpyAsync(ms.d_bflags, fl.data(), fl.size(), cudaMemcpyHostToDevice, op.stream), "copy brick flags");
+        ICC_CUDA(cudaMemcpyAsync(ms.d_desc, dv.data(), dv.size() * sizeof(BrickDesc), cudaMemcpyHostToDevice, op.stream),
+                 "copy brick list");
         ICC_CUDA(cudaMemcpyAsync(ms.d_edge, &ms.edge, sizeof(Edge), cudaMemcpyHostToDevice, op.stream), "copy edge");
-        ICC_CUDA(cudaStreamSynchronize(op.stream), "copy brick flags");
+        ICC_CUDA(cudaStreamSynchronize(op.stream), "copy brick list");
     }
     {
         int per_sm = 0;
@@ -1199,7 +1230,7 @@ void mixed_release(Op &op) {
     MixedState &ms = *op.mixed;
     if (ms.graph) cudaGraphExecDestroy(ms.graph);
     vecset_free(ms.v);
-    void *bufs[] = {ms.d_bmat, ms.d_bflags, ms.d_edge, ms.d_scale32, ms.d_scalars, ms.d_err, ms.d_state,
+    void *bufs[] = {ms.d_bmat, ms.d_desc, ms.d_edge, ms.d_scale32, ms.d_scalars, ms.d_err, ms.d_state,
                     ms.d_grid_ctr, ms.d_inst};
     for (void *p : bufs)
         if (p) cudaFree(p);
@@ -1226,20 +1257,17 @@ __global__ void mask_copy_kernel(long long n, const float *__restrict__ x, const
 }
 
 // The instance entry of system (op, v) with PCG state st (null: a plain apply of xin).
-static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, const float *xin, int brick0, int cta0, int ncta,
-                        float kfac) {
+static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, const float *xin, int cta0, int ncta, float kfac) {
     const MixedState &ms = *op.mixed;
     const bool ident = op.mask_mode == ICC_MASK_IDENTITY;
     TcInst I;
     std::memset(&I, 0, sizeof(I));
     I.g = op.g;
-    I.brick0 = brick0;
     I.cta0 = cta0;
     I.ncta = ncta;
     I.kfac = kfac;
     I.xin = xin ? xin : (ident ? v.xm32 : v.p32);
     I.scale = ms.d_scale32;
-    I.bflags = ms.d_bflags;
     I.edge = ms.d_edge;
     I.patch = v.patch32;
     I.mask = op.mask_mode != ICC_MASK_NONE ? op.d_mask : nullptr;
@@ -1256,10 +1284,10 @@ static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, const float
     return I;
 }
 
-static void launch_apply_tc(cudaStream_t s, const TcInst *d_insts, int ninst, int nbricks, const float4 *bmat, int *err,
-                            int num_sms) {
+static void launch_apply_tc(cudaStream_t s, const TcInst *d_insts, int ninst, int nbricks, const BrickDesc *d_desc,
+                            const float4 *bmat, int *err, int num_sms) {
     const int grid = std::min(num_sms, nbricks);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, s>>>(d_insts, ninst, nbricks, bmat, err);
+    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, s>>>(d_insts, ninst, nbricks, d_desc, bmat, err);
 }
 
 static cudaError_t launch_tail(cudaStream_t s, const TcInst *d_insts, int ninst, int grid, unsigned long long *ctr,
@@ -1286,9 +1314,9 @@ static int enqueue_apply_tc(Op &op, const float *x, float *y) {
         mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.ndof, x, op.d_mask, ms.v.xm32);
         xin = ms.v.xm32;
     }
-    const TcInst I = make_inst(op, ms.v, nullptr, xin, 0, 0, 0, 1.f);
+    const TcInst I = make_inst(op, ms.v, nullptr, xin, 0, 0, 1.f);
     ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
-    launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_bmat, ms.d_err, op.num_sms);
+    launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms);
     gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
                                                                        op.mask_mode, op.extra32(), y, nullptr, nullptr);
     ICC_CUDA(cudaGetLastError(), "tc apply launch");
@@ -1343,13 +1371,13 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     if (rc) return rc;
     MixedState &ms = *op.mixed;
     if ((rc = clear_flags(op.stream, ms.d_err, ms.d_grid_ctr))) return rc;
-    const TcInst I = make_inst(op, ms.v, nullptr, x, 0, 0, 0, 1.f);
+    const TcInst I = make_inst(op, ms.v, nullptr, x, 0, 0, 1.f);
     ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
     std::vector<cudaEvent_t> ev(3 * size_t(reps));
     for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(ev[3 * r], op.stream);
-        launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_bmat, ms.d_err, op.num_sms);
+        launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms);
         cudaEventRecord(ev[3 * r + 1], op.stream);
         gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
                                                                            ICC_MASK_NONE, op.extra32(), y, nullptr,
@@ -1449,6 +1477,7 @@ struct MixedItem {
 struct MixedBatch {
     cudaStream_t stream = nullptr;
     TcInst *d_inst = nullptr;
+    BrickDesc *d_desc = nullptr;   // all bricks of all systems, system by system
     PcgState *d_state = nullptr, *h_state = nullptr;
     double *d_scalars = nullptr, *h_scalars = nullptr;   // |b|^2 and |r|^2 per system
     int *d_err = nullptr, *h_err = nullptr;
@@ -1461,7 +1490,7 @@ struct MixedBatch {
     ~MixedBatch() {
         if (!owned) return;
         if (graph) cudaGraphExecDestroy(graph);
-        void *bufs[] = {d_inst, d_state, d_scalars, d_err, d_ctr};
+        void *bufs[] = {d_inst, d_desc, d_state, d_scalars, d_err, d_ctr};
         for (void *p : bufs)
             if (p) cudaFree(p);
         if (h_state) cudaFreeHost(h_state);
@@ -1662,7 +1691,7 @@ static int capture_graph(MixedBatch &bt, int check_every) {
     ICC_CUDA(cudaStreamBeginCapture(bt.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t ce = cudaSuccess;
     for (int i = 0; i < check_every && ce == cudaSuccess; ++i) {
-        launch_apply_tc(bt.stream, bt.d_inst, bt.ninst, bt.nbricks, bt.bmat, bt.d_err, bt.num_sms);
+        launch_apply_tc(bt.stream, bt.d_inst, bt.ninst, bt.nbricks, bt.d_desc, bt.bmat, bt.d_err, bt.num_sms);
         ce = launch_tail(bt.stream, bt.d_inst, bt.ninst, bt.tail_grid, bt.d_ctr, bt.d_err, bt.limit);
     }
     cudaError_t ee = cudaStreamEndCapture(bt.stream, &graph);
@@ -1693,6 +1722,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     MixedBatch bt;
     bt.stream = op.stream;
     bt.d_inst = ms.d_inst + 1;
+    bt.d_desc = ms.d_desc;
     bt.d_state = ms.d_state;
     bt.h_state = ms.h_state;
     bt.d_scalars = ms.d_scalars;
@@ -1708,7 +1738,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     bt.limit = ms.grid_wait_limit;
     bt.graph = ms.graph;
     if (!ms.graph || ms.graph_batch != check_every || ms.graph_limit != ms.grid_wait_limit) {
-        const TcInst I = make_inst(op, ms.v, ms.d_state, nullptr, 0, 0, bt.tail_grid, 1.f);
+        const TcInst I = make_inst(op, ms.v, ms.d_state, nullptr, 0, bt.tail_grid, 1.f);
         ICC_CUDA(cudaMemcpyAsync(bt.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
         bt.graph = ms.graph;
         if ((rc = capture_graph(bt, check_every))) return rc;
@@ -1772,7 +1802,7 @@ int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const s
     }
     std::vector<MixedItem> items(m);
     int nbricks = 0;
-    std::vector<int> brick0(m);
+    std::vector<BrickDesc> descs;
     for (size_t i = 0; i < m; ++i) {
         items[i].op = ops[i];
         items[i].v = vsets[i];
@@ -1782,9 +1812,11 @@ int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const s
         items[i].max_iter = max_iter[i];
         items[i].x_out = x[i];
         items[i].kfac = kfac[i];
-        brick0[i] = nbricks;
+        append_descs(*ops[i], (int)i, descs);
         nbricks += ops[i]->g.nbricks;
     }
+    if ((nbricks + ops[0]->num_sms - 1) / ops[0]->num_sms > kMaxListPerCta)
+        return set_error(ICC_BAD_ARG, "batched mixed solve: more than 2048 bricks per SM");
     const int cap = tail_capacity(*ops[0]);
     if ((int)m > cap) return set_error(ICC_BAD_ARG, "batched mixed solve: more systems than resident CTAs of the vector step");
     const std::vector<int> ncta = share_ctas(items, cap);
@@ -1796,7 +1828,8 @@ int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const s
     bt.num_sms = ops[0]->num_sms;
     bt.bmat = ops[0]->mixed->d_bmat;
     bt.limit = ops[0]->mixed->grid_wait_limit;
-    if ((rc = dalloc(&bt.d_inst, m, "alloc batch")) || (rc = dalloc(&bt.d_state, m, "alloc batch")) ||
+    if ((rc = dalloc(&bt.d_inst, m, "alloc batch")) || (rc = dalloc(&bt.d_desc, descs.size(), "alloc batch")) ||
+        (rc = dalloc(&bt.d_state, m, "alloc batch")) ||
         (rc = dalloc(&bt.d_scalars, m, "alloc batch")) || (rc = dalloc(&bt.d_err, 1, "alloc batch")) ||
         (rc = dalloc(&bt.d_ctr, 1, "alloc batch")))
         return rc;
@@ -1807,11 +1840,13 @@ int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const s
     int cta = 0;
     for (size_t i = 0; i < m; ++i) {
         if (vsets[i]->part_cap < ncta[i]) return set_error(ICC_BAD_ARG, "batched mixed solve: partial buffer too small");
-        tab[i] = make_inst(*ops[i], *vsets[i], bt.d_state + i, nullptr, brick0[i], cta, ncta[i], kfac[i]);
+        tab[i] = make_inst(*ops[i], *vsets[i], bt.d_state + i, nullptr, cta, ncta[i], kfac[i]);
         cta += ncta[i];
     }
     bt.tail_grid = cta;
     ICC_CUDA(cudaMemcpyAsync(bt.d_inst, tab.data(), m * sizeof(TcInst), cudaMemcpyHostToDevice, stream), "instance table");
+    ICC_CUDA(cudaMemcpyAsync(bt.d_desc, descs.data(), descs.size() * sizeof(BrickDesc), cudaMemcpyHostToDevice, stream),
+             "brick list");
     const int check_every = opts.check_every > 0 ? opts.check_every : 32;
     if ((rc = capture_graph(bt, check_every))) return rc;
     rc = run_mixed(bt, items, opts, nullptr);
