@@ -22,8 +22,11 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -63,6 +66,7 @@ struct BrickDesc {
     unsigned ext;   // ex_n | ey_n << 4 | ez_n << 8 | flags << 12
 };
 constexpr int kMaxListPerCta = 2048;   // bricks of one persistent CTA in one launch, at most
+constexpr int kMaxInst = 1024;         // systems of one batch, at most
 
 // One system of a mixed solve as the kernels see it: the operator data of its handle and its own
 // FP32 vectors.  A solve of one system is a batch of one; a batch of several (designs of uneven
@@ -283,6 +287,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     __shared__ int s_list[kMaxListPerCta];
     __shared__ int s_cnt[32];
     __shared__ int s_nlist;
+    __shared__ unsigned s_act[kMaxInst / 32];   // bit i: system i's solve goes on
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
              *fin = bars + 9;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -292,13 +297,19 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         const int G = gridDim.x, L = (nbricks - (int)blockIdx.x + G - 1) / G;
         constexpr int kW = kPtThreads / 32;
         if (tid == 0) s_nlist = 0;
+        for (int i = tid; i < kMaxInst / 32; i += kPtThreads) s_act[i] = 0u;
+        __syncthreads();
+        for (int i = tid; i < ninst; i += kPtThreads) {
+            const PcgState *st = insts[i].st;
+            if (!st || __ldcg(&st->status) == 0) atomicOr(&s_act[i >> 5], 1u << (i & 31));
+        }
         __syncthreads();
         for (int base = 0; base < L; base += kPtThreads) {
             const int k = base + tid;
             bool a = false;
             if (k < L) {
-                const PcgState *st = insts[desc[blockIdx.x + k * G].inst].st;
-                a = !st || __ldcg(&st->status) == 0;
+                const int si = ninst == 1 ? 0 : desc[blockIdx.x + k * G].inst;
+                a = (s_act[si >> 5] >> (si & 31)) & 1u;
             }
             const unsigned act = __ballot_sync(0xffffffffu, a);
             if (lane == 0) s_cnt[warp] = __popc(act);
@@ -350,9 +361,8 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         // patch rows (c, pz, py) of kPX floats; thread tid < 108 copies row tid, in 8-byte pieces
         // when the row is whole and starts on an even float (always when the x control-point
         // count is even), else float by float
-        auto load_patch = [&](int k, float *dst) {
+        auto load_patch = [&](int k, const BrickDesc &d, float *dst) {
             if (k < nmine && tid < 3 * kPZ * kPY) {
-                const BrickDesc d = desc[s_list[k]];
                 const TcInst &I = insts[d.inst];
                 const Geom &g = I.g;
                 const BrickBox bb = desc_box(d);
@@ -379,27 +389,38 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             }
             tc::cp_async_commit();
         };
-        // three patch buffers: the brick two ahead is fetched while one is built
-        load_patch(0, sP);
-        load_patch(1, sP + 3 * kPVol);
+        // three patch buffers: the brick two ahead is fetched while one is built; descriptors are
+        // read three bricks ahead (d1, d2, d3 = bricks it + 1, it + 2, it + 3)
+        auto get_desc = [&](int k) {
+            BrickDesc d{};
+            if (k < nmine) d = desc[s_list[k]];
+            return d;
+        };
+        const BrickDesc d0 = get_desc(0);
+        BrickDesc d1 = get_desc(1), d2 = get_desc(2), d3 = get_desc(3);
+        load_patch(0, d0, sP);
+        load_patch(1, d1, sP + 3 * kPVol);
         const int r = q * 32 + lane;
-        BrickDesc dn = desc[s_list[0]];
-        unsigned fl_next = desc_flags(dn);
-        float se_next = row_scale(insts[dn.inst], desc_box(dn), r);
+        BrickDesc dcur = d0;
+        unsigned fl_next = desc_flags(d0);
+        float se_next = row_scale(insts[d0.inst], desc_box(d0), r);
         for (int it = 0; it < nmine; ++it) {
             const int s = it & 1, pb = it % 3;
             const unsigned fl = fl_next;   // bit d: the brick's patch holds boundary points of d
             const float se = se_next;      // s_e k of this thread's element (0 outside the grid)
-            const BrickDesc d = dn;
+            const BrickDesc d = dcur;
             const TcInst &I = insts[d.inst];
             const Geom &g = I.g;
             const BrickBox bb = desc_box(d);
             if (it + 1 < nmine) {
-                dn = desc[s_list[it + 1]];
-                fl_next = desc_flags(dn);
-                se_next = row_scale(insts[dn.inst], desc_box(dn), r);
+                fl_next = desc_flags(d1);
+                se_next = row_scale(insts[d1.inst], desc_box(d1), r);
             }
-            load_patch(it + 2, sP + ((it + 2) % 3) * 3 * kPVol);
+            load_patch(it + 2, d2, sP + ((it + 2) % 3) * 3 * kPVol);
+            dcur = d1;
+            d1 = d2;
+            d2 = d3;
+            d3 = get_desc(it + 4);
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const float vm = valid ? se : 0.f;
             tc::cp_async_wait<2>();
@@ -800,30 +821,51 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
     const long long T = (long long)G * blockDim.x;
     const long long t0 = (long long)bid * blockDim.x + threadIdx.x;
     const long long n = 3 * g.nsc;
-    // A. Ap at every node and the five dot products
+    // A. Ap at every node and the five dot products; one warp per row (iy, iz) of control points,
+    // lanes along x, so the row's bricks are found once and neighbouring lanes read neighbouring
+    // partials
     double dA[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    // 32-bit index arithmetic: the set-up checks nsc < 2^31
-    const unsigned ucx = (unsigned)g.cx, ucy = (unsigned)g.cy;
-    for (long long nd = t0; nd < g.nsc; nd += T) {
-        const unsigned u = (unsigned)nd, q1 = u / ucx;
-        const int ix = int(u - q1 * ucx), iy = int(q1 % ucy), iz = int(q1 / ucy);
-        float sv[3];
-        node_partials(g, I.patch, ix, iy, iz, sv[0], sv[1], sv[2]);
+    const float *__restrict__ patch = I.patch;
+    {
+        const int lane = threadIdx.x & 31;
+        const int nrows = g.cy * g.cz;
+        const int wstride = (G * (int)blockDim.x) >> 5;
+        for (int row = (bid * (int)blockDim.x + (int)threadIdx.x) >> 5; row < nrows; row += wstride) {
+            const int iy = row % g.cy, iz = row / g.cy;
+            int by[2], ly[2], bz[2], lz[2];
+            const int nby = node_bricks(iy, kBY, g.nby, by, ly);
+            const int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
+            for (int ix = lane; ix < g.cx; ix += 32) {
+                const long long nd = (long long)row * g.cx + ix;
+                int bx[2], lx[2];
+                const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
+                float sv[3] = {0.f, 0.f, 0.f};
+                for (int a = 0; a < nbz; ++a)
+                    for (int q = 0; q < nby; ++q)
+                        for (int w = 0; w < nbx; ++w) {
+                            const size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
+                            const float *pq = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
+                            sv[0] += pq[0];
+                            sv[1] += pq[kPVol];
+                            sv[2] += pq[2 * kPVol];
+                        }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const long long idx = (long long)c * g.nsc + nd;
-            float v = sv[c];
-            if (I.sp.ptr) v += sparse_row(I.sp, idx, p, mask, mask_mode);
-            if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.f;
-            else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
-            ap[idx] = v;
-            const float ri = r[idx], iv = inv[idx];
-            const double av = double(v);
-            dA[0] += double(p[idx]) * av;
-            dA[1] += double(iv * ri) * av;
-            dA[2] += double(iv * v) * av;
-            dA[3] += double(ri) * av;
-            dA[4] += av * av;
+                for (int c = 0; c < 3; ++c) {
+                    const long long idx = (long long)c * g.nsc + nd;
+                    float v = sv[c];
+                    if (I.sp.ptr) v += sparse_row(I.sp, idx, p, mask, mask_mode);
+                    if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.f;
+                    else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
+                    ap[idx] = v;
+                    const float ri = r[idx], iv = inv[idx];
+                    const double av = double(v);
+                    dA[0] += double(p[idx]) * av;
+                    dA[1] += double(iv * ri) * av;
+                    dA[2] += double(iv * v) * av;
+                    dA[3] += double(ri) * av;
+                    dA[4] += av * av;
+                }
+            }
         }
     }
     block_sum5(dA);
@@ -1499,22 +1541,20 @@ struct MixedBatch {
     }
 };
 
-// Shares the fused vector step's CTAs among the systems: every system gets at least one, the
-// rest in proportion to its control points (no more than one per 256 of them).
-static std::vector<int> share_ctas(const std::vector<MixedItem> &items, int cap) {
+// Shares `cap` CTAs of the fused vector step among the systems: every system gets at least one,
+// the rest in proportion to its control points (mode 0) or in equal parts (mode 1), never more
+// than one per 256 control points.
+static std::vector<int> share_ctas(const std::vector<MixedItem> &items, int cap, int mode = 0) {
     const size_t m = items.size();
     std::vector<int> n(m, 1);
     long long tot = 0;
     for (const auto &it : items) tot += it.op->g.nsc;
-    int used = int(m);
     for (size_t i = 0; i < m; ++i) {
         const long long need = (items[i].op->g.nsc + kTailThreads - 1) / kTailThreads;
-        const long long want = (long long)((double)(cap - (int)m) * (double)items[i].op->g.nsc / (double)tot);
-        const int add = (int)std::max(0LL, std::min(need - 1, want));
-        n[i] += add;
-        used += add;
+        const double frac = mode == 0 ? (double)items[i].op->g.nsc / (double)tot : 1.0 / (double)m;
+        const long long want = (long long)((double)(cap - (int)m) * frac);
+        n[i] += (int)std::max(0LL, std::min(need - 1, want));
     }
-    (void)used;
     return n;
 }
 
@@ -1527,22 +1567,17 @@ static std::vector<int> share_ctas(const std::vector<MixedItem> &items, int cap)
 // direction is kept.  A system stops when its FP64 residual meets its tolerance (the reference's
 // stopping rule, rust/src/solver.rs:56-58, evaluated on the true residual), on breakdown or NaN,
 // or when its iteration budget or progress runs out.
-static int run_mixed(MixedBatch &bt, std::vector<MixedItem> &items, const icc_solve_opts &opts, int64_t *launches_out) {
+constexpr int64_t kMaxSegment = 512;  // FP32 iterations between residual replacements at most
+
+// Initial state of every system: x = 0, r = b, |b|, the FP32 recurrence armed for residual
+// replacement by the factor delta (0: never, as the autotuner runs it), tolerance tol of the
+// system (trial: 0, so no system stops while candidates are timed).
+static int init_items(MixedBatch &bt, std::vector<MixedItem> &items, double delta, int check_every, bool trial,
+                      int64_t &launches) {
     cudaStream_t s = bt.stream;
     const size_t m = items.size();
-    // 0.6: a replacement every ~75 iterations at 128x64x64 keeps the FP32 recurrence close to the
-    // FP64 iteration count (1,350-1,410 vs 1,337 over four seeds; 0.1 gave up to 1,820)
-    const double delta = opts.inner_tol > 0.0 ? opts.inner_tol : 0.6;
-    const int max_updates = opts.max_outer > 0 ? opts.max_outer : 1000;
-    const int check_every = opts.check_every > 0 ? opts.check_every : 32;
-    constexpr int64_t kMaxSegment = 512;  // FP32 iterations between residual replacements at most
-    // give up after the FP32 recurrence has gained eight decades (8 ln 0.1 / ln delta replacements)
-    // without a 10% improvement of the true residual
-    const int max_no_progress = std::max(8, (int)std::ceil(8.0 * std::log(0.1) / std::log(std::fmin(delta, 0.99))));
-    int64_t launches = 0;
     int rc;
     if ((rc = clear_flags(s, bt.d_err, bt.d_ctr))) return rc;
-    // initialisation: x = 0, r = b, |b| per system
     for (size_t i = 0; i < m; ++i) {
         MixedItem &it = items[i];
         Op &op = *it.op;
@@ -1579,9 +1614,9 @@ static int run_mixed(MixedBatch &bt, std::vector<MixedItem> &items, const icc_so
         ir_to_f32_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.r64, v.rhs32, bt.d_scalars + i);
         pcg_init_kernel<float><<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.rhs32, v.inv32, v.x32, v.r32, v.p32,
                                                                      op.d_partials, pm);
-        pcg_init_finalize<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_state + i, it.tol,
-                                                    (long long)it.max_iter);
-        ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, 1.0, delta, kMaxSegment, check_every);
+        pcg_init_finalize<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_state + i, trial ? 0.0 : it.tol,
+                                                    trial ? (1LL << 40) : (long long)it.max_iter);
+        ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, 1.0, trial ? 0.0 : delta, kMaxSegment, check_every);
         launches += 4;
         if (op.mask_mode == ICC_MASK_IDENTITY) {
             mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.p32, op.d_mask, v.xm32);
@@ -1589,6 +1624,23 @@ static int run_mixed(MixedBatch &bt, std::vector<MixedItem> &items, const icc_so
         }
     }
     ICC_CUDA(cudaGetLastError(), "mixed init");
+    return ICC_OK;
+}
+
+static int run_mixed(MixedBatch &bt, std::vector<MixedItem> &items, const icc_solve_opts &opts, int64_t *launches_out) {
+    cudaStream_t s = bt.stream;
+    const size_t m = items.size();
+    // 0.6: a replacement every ~75 iterations at 128x64x64 keeps the FP32 recurrence close to the
+    // FP64 iteration count (1,350-1,410 vs 1,337 over four seeds; 0.1 gave up to 1,820)
+    const double delta = opts.inner_tol > 0.0 ? opts.inner_tol : 0.6;
+    const int max_updates = opts.max_outer > 0 ? opts.max_outer : 1000;
+    const int check_every = opts.check_every > 0 ? opts.check_every : 32;
+    // give up after the FP32 recurrence has gained eight decades (8 ln 0.1 / ln delta replacements)
+    // without a 10% improvement of the true residual
+    const int max_no_progress = std::max(8, (int)std::ceil(8.0 * std::log(0.1) / std::log(std::fmin(delta, 0.99))));
+    int64_t launches = 0;
+    int rc;
+    if ((rc = init_items(bt, items, delta, check_every, false, launches))) return rc;
 
     int64_t launched = 0, max_budget = 0;
     for (const auto &it : items) max_budget = std::max(max_budget, it.max_iter);
@@ -1761,6 +1813,119 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     return items[0].status;
 }
 
+// ---- autotuner of the batched solve -------------------------------------------------------------
+// The batch's free choices are how many CTAs of the fused vector step run per SM (its grid barrier
+// needs them all resident: 1, 2 or 4) and how they are shared among the systems (in proportion to
+// their control points, or in equal parts).  Each candidate is timed on the batch itself: the
+// systems are initialised with residual replacement off and no tolerance, a graph of kTuneIters
+// iterations runs once to warm up and once under CUDA events, and the fastest per iteration wins.
+// Choices are kept per batch shape (the systems' grid sizes and mask modes, and the SM count) for
+// the process, and in the JSON file named by the environment variable ICC_TUNE_CACHE when it is
+// set, so other processes reuse them.
+struct TuneChoice {
+    int per_sm = 4, share = 0;
+    double us_per_iter = 0.0;
+};
+constexpr int kTuneIters = 16;
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneChoice> g_tune;
+static bool g_tune_loaded = false;
+
+static std::string tune_key(const std::vector<MixedItem> &items, int sms) {
+    std::string k = "sms" + std::to_string(sms);
+    for (const auto &it : items)
+        k += ";" + std::to_string(it.op->g.nx) + "x" + std::to_string(it.op->g.ny) + "x" + std::to_string(it.op->g.nz) +
+             "m" + std::to_string(it.op->mask_mode);
+    return k;
+}
+
+// The cache file: one JSON object {"key": [per_sm, share, us_per_iter], ...}, one entry a line.
+static void tune_load() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char *path = std::getenv("ICC_TUNE_CACHE");
+    if (!path) return;
+    std::FILE *f = std::fopen(path, "r");
+    if (!f) return;
+    char line[65536];
+    while (std::fgets(line, sizeof line, f)) {
+        char *q0 = std::strchr(line, '"');
+        char *q1 = q0 ? std::strchr(q0 + 1, '"') : nullptr;
+        char *br = q1 ? std::strchr(q1, '[') : nullptr;
+        if (!br) continue;
+        TuneChoice c;
+        if (std::sscanf(br + 1, "%d , %d , %lf", &c.per_sm, &c.share, &c.us_per_iter) == 3)
+            g_tune[std::string(q0 + 1, q1)] = c;
+    }
+    std::fclose(f);
+}
+
+static void tune_save() {
+    const char *path = std::getenv("ICC_TUNE_CACHE");
+    if (!path) return;
+    std::FILE *f = std::fopen(path, "w");
+    if (!f) return;
+    std::fprintf(f, "{\n");
+    size_t k = 0;
+    for (const auto &kv : g_tune)
+        std::fprintf(f, "  \"%s\": [%d, %d, %.3f]%s\n", kv.first.c_str(), kv.second.per_sm, kv.second.share,
+                     kv.second.us_per_iter, ++k < g_tune.size() ? "," : "");
+    std::fprintf(f, "}\n");
+    std::fclose(f);
+}
+
+static int upload_table(MixedBatch &bt, std::vector<MixedItem> &items, const std::vector<int> &ncta) {
+    std::vector<TcInst> tab(items.size());
+    int cta = 0;
+    for (size_t i = 0; i < items.size(); ++i) {
+        if (items[i].v->part_cap < ncta[i]) return set_error(ICC_BAD_ARG, "batched mixed solve: partial buffer too small");
+        tab[i] = make_inst(*items[i].op, *items[i].v, bt.d_state + i, nullptr, cta, ncta[i], items[i].kfac);
+        cta += ncta[i];
+    }
+    bt.tail_grid = cta;
+    ICC_CUDA(cudaMemcpyAsync(bt.d_inst, tab.data(), tab.size() * sizeof(TcInst), cudaMemcpyHostToDevice, bt.stream),
+             "instance table");
+    return ICC_OK;
+}
+
+static int autotune(MixedBatch &bt, std::vector<MixedItem> &items, int max_per_sm, TuneChoice &best) {
+    cudaEvent_t e0, e1;
+    ICC_CUDA(cudaEventCreate(&e0), "event");
+    ICC_CUDA(cudaEventCreate(&e1), "event");
+    best.us_per_iter = INFINITY;
+    int rc = ICC_OK;
+    for (int per_sm : {1, 2, 4}) {
+        if (per_sm > max_per_sm || rc) continue;
+        for (int share = 0; share < 2 && !rc; ++share) {
+            const std::vector<int> ncta = share_ctas(items, per_sm * bt.num_sms, share);
+            int64_t l = 0;
+            if ((rc = upload_table(bt, items, ncta)) || (rc = capture_graph(bt, kTuneIters)) ||
+                (rc = init_items(bt, items, 0.0, kTuneIters, true, l)))
+                break;
+            cudaGraphLaunch(bt.graph, bt.stream);
+            cudaEventRecord(e0, bt.stream);
+            cudaGraphLaunch(bt.graph, bt.stream);
+            cudaEventRecord(e1, bt.stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(e, "autotune");
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double us = 1e3 * ms / kTuneIters;
+            if (us < best.us_per_iter) {
+                best.us_per_iter = us;
+                best.per_sm = per_sm;
+                best.share = share;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
 // Several systems at once: systems m of the call are (ops[m], vsets[m]) with right-hand side b[m]
 // (device), Jacobi diagonal diag[m] (device, null: the operator's own), tolerance tol[m] and
 // budget max_iter[m]; solutions into x[m] (device).  All operators must be on one device and have
@@ -1818,8 +1983,8 @@ int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const s
     if ((nbricks + ops[0]->num_sms - 1) / ops[0]->num_sms > kMaxListPerCta)
         return set_error(ICC_BAD_ARG, "batched mixed solve: more than 2048 bricks per SM");
     const int cap = tail_capacity(*ops[0]);
-    if ((int)m > cap) return set_error(ICC_BAD_ARG, "batched mixed solve: more systems than resident CTAs of the vector step");
-    const std::vector<int> ncta = share_ctas(items, cap);
+    if ((int)m > cap || (int)m > kMaxInst)
+        return set_error(ICC_BAD_ARG, "batched mixed solve: more systems than resident CTAs of the vector step");
     MixedBatch bt;
     bt.owned = true;
     bt.stream = stream;
@@ -1836,17 +2001,31 @@ int mixed_solve_batch(cudaStream_t stream, const std::vector<Op *> &ops, const s
     ICC_CUDA(cudaMallocHost((void **)&bt.h_state, m * sizeof(PcgState)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&bt.h_scalars, m * sizeof(double)), "alloc pinned");
     ICC_CUDA(cudaMallocHost((void **)&bt.h_err, sizeof(int)), "alloc pinned");
-    std::vector<TcInst> tab(m);
-    int cta = 0;
-    for (size_t i = 0; i < m; ++i) {
-        if (vsets[i]->part_cap < ncta[i]) return set_error(ICC_BAD_ARG, "batched mixed solve: partial buffer too small");
-        tab[i] = make_inst(*ops[i], *vsets[i], bt.d_state + i, nullptr, cta, ncta[i], kfac[i]);
-        cta += ncta[i];
-    }
-    bt.tail_grid = cta;
-    ICC_CUDA(cudaMemcpyAsync(bt.d_inst, tab.data(), m * sizeof(TcInst), cudaMemcpyHostToDevice, stream), "instance table");
     ICC_CUDA(cudaMemcpyAsync(bt.d_desc, descs.data(), descs.size() * sizeof(BrickDesc), cudaMemcpyHostToDevice, stream),
              "brick list");
+    // the vector step's CTAs: tuned once per batch shape (a single system takes them all)
+    TuneChoice ch;
+    ch.per_sm = ops[0]->mixed->tail_per_sm;
+    if (m > 1) {
+        const std::string key = tune_key(items, bt.num_sms);
+        bool have = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            tune_load();
+            auto it = g_tune.find(key);
+            if (it != g_tune.end() && it->second.per_sm <= ops[0]->mixed->tail_per_sm) {
+                ch = it->second;
+                have = true;
+            }
+        }
+        if (!have) {
+            if ((rc = autotune(bt, items, ops[0]->mixed->tail_per_sm, ch))) return rc;
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune[key] = ch;
+            tune_save();
+        }
+    }
+    if ((rc = upload_table(bt, items, share_ctas(items, ch.per_sm * bt.num_sms, ch.share)))) return rc;
     const int check_every = opts.check_every > 0 ? opts.check_every : 32;
     if ((rc = capture_graph(bt, check_every))) return rc;
     rc = run_mixed(bt, items, opts, nullptr);
