@@ -65,7 +65,7 @@ struct BrickDesc {
     unsigned xyz;   // bx | by << 11 | bz << 22
     unsigned ext;   // ex_n | ey_n << 4 | ez_n << 8 | flags << 12
 };
-constexpr int kMaxListPerCta = 2048;   // bricks of one persistent CTA in one launch, at most
+constexpr int kMaxListPerCta = 1024;   // bricks of one persistent CTA in one launch, at most
 constexpr int kMaxInst = 1024;         // systems of one batch, at most
 
 // One system of a mixed solve as the kernels see it: the operator data of its handle and its own
@@ -156,7 +156,9 @@ constexpr int kAloFl = kTcM * kTcK;    // A_lo slot (shared memory, canonical K-
 constexpr uint32_t kALbo = (kTcM / 8) * 128;  // bytes between K-adjacent core matrices of A_lo
 constexpr uint32_t kPtTmemCols = 512;
 constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
-constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * 3 * kPVol + 2 * kZFl + 3 * kPVol) * 4;  // 206,592 B
+constexpr int kWPat = 3 * kPY * kPX;           // a builder warp's patch: its 3 z-rows x 6 x 10 of one component
+constexpr int kPatBuf = kRoleWarps * kWPat;     // one patch buffer of all builder warps
+constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * kPatBuf + 2 * kZFl + 3 * kPVol) * 4;  // 219,552 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
 // Each test may sleep up to kWaitSleepNs; with kWaitLimit tests a wait gives up after at most
@@ -192,41 +194,41 @@ __device__ __forceinline__ BrickBox desc_box(const BrickDesc &d) {
 
 __device__ __forceinline__ unsigned desc_flags(const BrickDesc &d) { return (d.ext >> 12) & 7u; }
 
-// V = E' u on the boundary control points of direction D inside the patch P (3 x kPZ x kPY x kPX,
-// patch origin o along D, ext of its control points inside the grid); line t along D (t < the
-// number of lines) is handled by thread t.  Every control point that a boundary value needs lies
-// in the patch: the set-up checks that E couples only control points of a common element.
+// V = E' u on the boundary control points of direction D in a builder warp's own patch
+// P[3][kPY][kPX] (the z-window of its z-layer; origin o along D, ext of its control points inside
+// the grid); the warp's lanes take the lines along D.  The window of the warp's elements holds
+// every control point a boundary value needs: the set-up checks that E couples only control
+// points of a common element.
 template <int D>
-__device__ __forceinline__ void edge_in(float *P, const Edge &E, int o, int ext, int t) {
-    constexpr int LA = D == 0 ? kPY : kPX;   // extent of the line index that runs fastest
-    constexpr int LB = D == 2 ? kPY : kPZ;
+__device__ __forceinline__ void edge_in_warp(float *P, const Edge &E, int o, int ext, int lane) {
+    constexpr int LA = D == 0 ? kPY : kPX;
+    constexpr int LB = D == 2 ? kPY : 3;
     constexpr int stride = D == 0 ? 1 : (D == 1 ? kPX : kPX * kPY);
-    if (t >= 3 * LA * LB) return;
-    const int c = t / (LA * LB), w = t - c * (LA * LB), a1 = w % LA, a2 = w / LA;
-    const int base = D == 0 ? c * kPVol + (a2 * kPY + a1) * kPX
-                            : (D == 1 ? c * kPVol + a2 * (kPY * kPX) + a1 : c * kPVol + a2 * kPX + a1);
     const int nb = E.nb[D];
-    float u[4], v[4];
-    int loc[4];
+    for (int t = lane; t < LA * LB; t += 32) {
+        const int a1 = t % LA, a2 = t / LA;
+        const int base = D == 0 ? (a2 * kPY + a1) * kPX : (D == 1 ? a2 * (kPY * kPX) + a1 : a2 * kPX + a1);
+        float u[4], v[4];
+        int loc[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int l = a < nb ? E.id[D][a] - o : -1;
-        loc[a] = (l >= 0 && l < ext) ? l : -1;
-        u[a] = loc[a] >= 0 ? P[base + loc[a] * stride] : 0.f;
+        for (int a = 0; a < 4; ++a) {
+            const int l = a < nb ? E.id[D][a] - o : -1;
+            loc[a] = (l >= 0 && l < ext) ? l : -1;
+            u[a] = loc[a] >= 0 ? P[base + loc[a] * stride] : 0.f;
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            float acc = 0.f;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) acc = fmaf(E.e[D][a][b], u[a], acc);
+            v[b] = acc;
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            if (loc[b] >= 0) P[base + loc[b] * stride] = v[b];
     }
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        float acc = 0.f;
-#pragma unroll
-        for (int a = 0; a < 4; ++a) acc = fmaf(E.e[D][a][b], u[a], acc);
-        v[b] = acc;
-    }
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-        if (loc[b] >= 0) P[base + loc[b] * stride] = v[b];
 }
 
-// s_e times the system's K_u factor for brick row r (element lx + 8 ly + 32 lz), 0 outside the grid
 // W <- E W on the boundary control points of direction D of a brick's node partials P (patch
 // layout, origin o along D, ext of them inside the grid); line t along D is handled by thread t.
 // E couples only control points of a common element, so the partials of one brick transform on
@@ -277,8 +279,8 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
     float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
-    float *sP = sAlo + 2 * kAloFl;        // [3][3 * kPVol] input patches
-    float *sZb = sP + 3 * 3 * kPVol;      // [2][kZFl] per-layer node partials, by brick parity
+    float *sP = sAlo + 2 * kAloFl;        // [3][kPatBuf] input patches, each builder warp its own part
+    float *sZb = sP + 3 * kPatBuf;        // [2][kZFl] per-layer node partials, by brick parity
     float *sW = sZb + 2 * kZFl;           // [3 * kPVol] node partials of a boundary brick (E applied)
     __shared__ __align__(8) uint64_t bars[10];
     __shared__ uint32_t tmem_base;
@@ -354,23 +356,25 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
 
     if (warp < kRoleWarps) {
         // ------------------------------ builders ------------------------------
-        // warp = 4 c + q: component c of the 32 elements of z-layer q (TMEM lanes 32 q ..)
+        // warp = 4 c + q: component c of the 32 elements of z-layer q (TMEM lanes 32 q ..).  Each
+        // warp fetches and transforms its own patch (component c, z-rows q .. q + 2: exactly the
+        // control points of its elements), so the builders never wait for each other.
         const int c = warp >> 2, q = warp & 3;
         const int lx = lane & 7, ly = lane >> 3;
-        const int base = c * kPVol + (q * kPY + ly) * kPX + lx;
-        // patch rows (c, pz, py) of kPX floats; thread tid < 108 copies row tid, in 8-byte pieces
-        // when the row is whole and starts on an even float (always when the x control-point
-        // count is even), else float by float
+        const unsigned FULLW = 0xffffffffu;
+        // lane l < 18 copies row l = (pz, py) of kPX floats, in 8-byte pieces when the row is whole
+        // and starts on an even float (always when the x control-point count is even), else float
+        // by float
         auto load_patch = [&](int k, const BrickDesc &d, float *dst) {
-            if (k < nmine && tid < 3 * kPZ * kPY) {
+            if (k < nmine && lane < 3 * kPY) {
                 const TcInst &I = insts[d.inst];
                 const Geom &g = I.g;
                 const BrickBox bb = desc_box(d);
-                const int rc = tid / (kPZ * kPY), py = tid % kPY, pz = (tid / kPY) % kPZ;
-                const int gy = bb.y0 + py, gz = bb.z0 + pz;
-                float *drow = dst + tid * kPX;
+                const int py = lane % kPY, pz = lane / kPY;
+                const int gy = bb.y0 + py, gz = bb.z0 + q + pz;
+                float *drow = dst + lane * kPX;
                 if (gy < g.cy && gz < g.cz) {
-                    const long long off = (long long)rc * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
+                    const long long off = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
                     const float *srow = I.xin + off;
                     if (bb.x0 + kPX <= g.cx && !(off & 1)) {
 #pragma unroll
@@ -389,6 +393,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             }
             tc::cp_async_commit();
         };
+        float *sPw = sP + warp * kWPat;   // this warp's part of each patch buffer
         // three patch buffers: the brick two ahead is fetched while one is built; descriptors are
         // read three bricks ahead (d1, d2, d3 = bricks it + 1, it + 2, it + 3)
         auto get_desc = [&](int k) {
@@ -398,8 +403,8 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         };
         const BrickDesc d0 = get_desc(0);
         BrickDesc d1 = get_desc(1), d2 = get_desc(2), d3 = get_desc(3);
-        load_patch(0, d0, sP);
-        load_patch(1, d1, sP + 3 * kPVol);
+        load_patch(0, d0, sPw);
+        load_patch(1, d1, sPw + kPatBuf);
         const int r = q * 32 + lane;
         BrickDesc dcur = d0;
         unsigned fl_next = desc_flags(d0);
@@ -416,7 +421,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
                 fl_next = desc_flags(d1);
                 se_next = row_scale(insts[d1.inst], desc_box(d1), r);
             }
-            load_patch(it + 2, d2, sP + ((it + 2) % 3) * 3 * kPVol);
+            load_patch(it + 2, d2, sPw + ((it + 2) % 3) * kPatBuf);
             dcur = d1;
             d1 = d2;
             d2 = d3;
@@ -425,30 +430,31 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             const float vm = valid ? se : 0.f;
             tc::cp_async_wait<2>();
             const bool ok = it < 2 || pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
-            // brick it's patch has landed for every builder; all builders leave together on abort
-            if (tc::named_sync_or(1, kRoleThreads, !ok || s_abort != 0)) break;
+            // the warp leaves together on abort (nothing of the other warps waits for it here)
+            if (!__all_sync(FULLW, ok && s_abort == 0)) break;
+            __syncwarp();   // every lane's rows of this brick have landed
+            float *Pw = sPw + pb * kPatBuf;
             if (fl) {   // V = E' u on the boundary control planes, one direction after the other
-                float *P = sP + pb * 3 * kPVol;
                 const Edge &E = *I.edge;
                 if (fl & 1u) {
-                    edge_in<0>(P, E, bb.x0, min(kPX, g.cx - bb.x0), tid);
-                    tc::named_sync(1, kRoleThreads);
+                    edge_in_warp<0>(Pw, E, bb.x0, min(kPX, g.cx - bb.x0), lane);
+                    __syncwarp();
                 }
                 if (fl & 2u) {
-                    edge_in<1>(P, E, bb.y0, min(kPY, g.cy - bb.y0), tid);
-                    tc::named_sync(1, kRoleThreads);
+                    edge_in_warp<1>(Pw, E, bb.y0, min(kPY, g.cy - bb.y0), lane);
+                    __syncwarp();
                 }
                 if (fl & 4u) {
-                    edge_in<2>(P, E, bb.z0, min(kPZ, g.cz - bb.z0), tid);
-                    tc::named_sync(1, kRoleThreads);
+                    edge_in_warp<2>(Pw, E, bb.z0 + q, min(3, g.cz - bb.z0 - q), lane);
+                    __syncwarp();
                 }
             }
             tc::fence_after_sync();
-            const float *Pc = sP + pb * 3 * kPVol + base;
+            const float *Pc = Pw + ly * kPX + lx;
             float v[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) v[a] = Pc[(a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
-            // Element-local shift: K_u maps a constant per-component field to zero, so subtracting
+        // Element-local shift: K_u maps a constant per-component field to zero, so subtracting
             // the element's centre control value changes nothing in exact arithmetic while the
             // split operands carry only the variation across the element; the TF32 splitting
             // error then scales with that variation instead of with |u| (smooth, low-energy
@@ -473,7 +479,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(&a_full[s]);
-            tc::named_sync(1, kRoleThreads);   // everyone is done with this patch before it is refilled
+            __syncwarp();   // the warp is done with this patch before it is refilled
         }
         tc::cp_async_wait<0>();
     } else if (warp < 2 * kRoleWarps) {
