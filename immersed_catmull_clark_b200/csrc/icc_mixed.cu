@@ -17,6 +17,8 @@
 // the FP64 solution accumulates its updates and the FP64 true residual b - A x (FP64 apply)
 // replaces the FP32 residual whenever it has fallen by a factor delta; the solve stops on the
 // FP64 true residual.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -73,10 +75,10 @@ constexpr int kMaxInst = 1024;         // systems of one batch, at most
 // sizes, or load cases of one operator) runs every iteration as one persistent apply over all
 // bricks of all systems and one fused vector step whose CTAs are shared out among the systems.
 struct TcInst {
+    CUtensorMap tmap;            // the apply input pin as a 4-D tensor (x, y, z, component), for TMA
     Geom g;
     int cta0, ncta;              // CTAs of the fused vector step that serve it
     float kfac;                  // the system's K_u = kfac * the batch's K_u (same element shape)
-    const float *xin;            // input of the brick apply (p, or the masked copy pm)
     const float *scale;          // s_e (FP32)
     const Edge *edge;
     float *patch;                // brick partials [nbricks][3][kPVol]
@@ -84,7 +86,9 @@ struct TcInst {
     int mask_mode;
     Sparse<float> sp;
     const float *inv;
-    float *x, *r, *p, *pm, *ap;
+    float *x, *r, *p, *ap;
+    float *pin;                  // the brick apply's input: the masked p, rows padded to cxp
+    int cxp;
     double *part;                // [7][ncta] partial sums of the fused vector step
     PcgState *st;                // null for a plain apply: every brick is active
 };
@@ -92,7 +96,12 @@ struct TcInst {
 // The FP32 and FP64 vectors and the PCG state of one system of a mixed solve.
 struct VecSet {
     float *patch32 = nullptr, *rhs32 = nullptr, *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *ap32 = nullptr,
-          *xm32 = nullptr, *inv32 = nullptr;   // xm32: masked input of the brick apply (ICC_MASK_IDENTITY)
+          *inv32 = nullptr;
+    // the brick apply's input [3][cz][cy][cxp] (rows padded to a multiple of 4 floats, so every row
+    // starts on 16 bytes as TMA needs) and its tensor map
+    float *pin32 = nullptr;
+    int cxp = 0;
+    CUtensorMap tmap{};
     double *x64 = nullptr, *r64 = nullptr, *y64 = nullptr;
     double *part = nullptr;  // [7][tail CTAs]
     int part_cap = 0;
@@ -128,12 +137,15 @@ struct MixedState {
 // ---- persistent, warp-specialised tensor-core brick apply ------------------------------------
 // One CTA per SM walks the bricks blockIdx.x, blockIdx.x + gridDim.x, ... of the batch's brick
 // numbering (all bricks of all systems), skipping systems whose solve has stopped.  Roles
-// (25 warps):
-//   warps 0-11 (builders, warp 4 c + q: component c of z-layer q): fetch the input patch two
-//     bricks ahead with cp.async; on bricks at the grid's ends transform the patch by E' (the
-//     boundary extraction); gather each element's 27 values of component c, shift them by the
-//     element's centre value and scale by s_e, split into TF32 hi/lo and store A_hi into TMEM
-//     (row m = element m = lane m) and A_lo into shared memory, in two A slots;
+// (26 warps):
+//   warp 25 (loader): one thread fetches the input patch of each brick (3 x 6 x 6 x 12 control
+//     values, zero outside the grid) with one TMA copy, up to three bricks ahead, into one of four
+//     patch buffers; the warp transforms the patches of bricks at the grid's ends by E' (the
+//     boundary extraction) and hands each buffer to the builders through an mbarrier;
+//   warps 0-11 (builders, warp 4 c + q: component c of z-layer q): gather each element's 27
+//     values of component c from the shared patch, shift them by the element's centre value and
+//     scale by s_e, split into TF32 hi/lo and store A_hi into TMEM (row m = element m = lane m)
+//     and A_lo into shared memory, in two A slots;
 //   warp 24 (MMA, one thread): holds B = K_u hi/lo in shared memory and issues the 36
 //     tcgen05.mma of a brick (A_lo B_hi from shared memory, A_hi B_lo and A_hi B_hi with A from
 //     TMEM) into one of two TMEM accumulators;
@@ -141,24 +153,31 @@ struct MixedState {
 //     release them, sum the element results per patch node with warp shuffles (x, y) and a
 //     shared buffer (z), transform the node partials of bricks at the grid's ends by E, and
 //     write the brick partials.
-// mbarriers: a_full/a_empty (A slots), d_full/d_empty (two accumulator buffers), b_full, fin.
+// mbarriers: t_full (TMA copies), p_full/p_empty (patch buffers), a_full/a_empty (A slots),
+// d_full/d_empty (two accumulator buffers), b_full, fin.
 // Every wait is bounded.  On time-out the waiting thread raises a shared abort flag; every other
 // wait then returns false at once.  The builders and the epilogue decide at a barrier that ORs
 // the flag over the role, so all threads of a role leave their loop at the same brick; the MMA
 // thread stops issuing, then commits once more and waits (bounded) for that commit, so no MMA
 // of the CTA is in flight when TMEM is released.  The host reports ICC_TIMEOUT.
-constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24
+constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24, loader: 25
 constexpr int kRoleThreads = kRoleWarps * 32;
-constexpr int kPtThreads = (2 * kRoleWarps + 1) * 32;
+constexpr int kMmaWarp = 2 * kRoleWarps, kLoaderWarp = 2 * kRoleWarps + 1;
+constexpr int kPtThreads = (2 * kRoleWarps + 2) * 32;
 constexpr int kColSlot = kTcK;         // A_hi slot s: TMEM columns s*96 + [0,96)
 constexpr int kColD = 2 * kColSlot;    // accumulator buffer d: TMEM columns 192 + d*96 + [0,96)
 constexpr int kAloFl = kTcM * kTcK;    // A_lo slot (shared memory, canonical K-major): floats
 constexpr uint32_t kALbo = (kTcM / 8) * 128;  // bytes between K-adjacent core matrices of A_lo
 constexpr uint32_t kPtTmemCols = 512;
 constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
-constexpr int kWPat = 3 * kPY * kPX;           // a builder warp's patch: its 3 z-rows x 6 x 10 of one component
-constexpr int kPatBuf = kRoleWarps * kWPat;     // one patch buffer of all builder warps
-constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + 3 * kPatBuf + 2 * kZFl + 3 * kPVol) * 4;  // 219,552 B
+constexpr int kPXs = 12;                        // x extent of an input patch row in shared memory (48 B)
+constexpr int kPVolS = kPZ * kPY * kPXs;        // per component
+constexpr uint32_t kPatchBytes = 3 * kPVolS * 4;   // one TMA box: 5,184 B
+constexpr int kPatBuf = 1312;                   // floats per patch buffer (5,248 B: 128-byte aligned)
+constexpr int kNPatch = 4;                      // patch buffers (the loader runs up to 3 bricks ahead)
+constexpr int kLoadAhead = 2;                   // bricks whose copies are in flight while one is finished
+static_assert(kPatBuf * 4 >= (int)kPatchBytes && (kPatBuf * 4) % 128 == 0, "patch buffer");
+constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + kNPatch * kPatBuf + 2 * kZFl + 3 * kPVol) * 4;  // 214,624 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
 // Each test may sleep up to kWaitSleepNs; with kWaitLimit tests a wait gives up after at most
@@ -194,39 +213,38 @@ __device__ __forceinline__ BrickBox desc_box(const BrickDesc &d) {
 
 __device__ __forceinline__ unsigned desc_flags(const BrickDesc &d) { return (d.ext >> 12) & 7u; }
 
-// V = E' u on the boundary control points of direction D in a builder warp's own patch
-// P[3][kPY][kPX] (the z-window of its z-layer; origin o along D, ext of its control points inside
-// the grid); the warp's lanes take the lines along D.  The window of the warp's elements holds
-// every control point a boundary value needs: the set-up checks that E couples only control
-// points of a common element.
+// V = E' u on the boundary control points of direction D inside the patch P (3 x kPZ x kPY x kPXs,
+// patch origin o along D, ext of its control points inside the grid); line t along D (t < the
+// number of lines) is handled by thread t.  Every control point that a boundary value needs lies
+// in the patch: the set-up checks that E couples only control points of a common element.
 template <int D>
-__device__ __forceinline__ void edge_in_warp(float *P, const Edge &E, int o, int ext, int lane) {
-    constexpr int LA = D == 0 ? kPY : kPX;
-    constexpr int LB = D == 2 ? kPY : 3;
-    constexpr int stride = D == 0 ? 1 : (D == 1 ? kPX : kPX * kPY);
+__device__ __forceinline__ void edge_in(float *P, const Edge &E, int o, int ext, int t) {
+    constexpr int LA = D == 0 ? kPY : kPX;   // extent of the line index that runs fastest
+    constexpr int LB = D == 2 ? kPY : kPZ;
+    constexpr int stride = D == 0 ? 1 : (D == 1 ? kPXs : kPXs * kPY);
+    if (t >= 3 * LA * LB) return;
+    const int c = t / (LA * LB), w = t - c * (LA * LB), a1 = w % LA, a2 = w / LA;
+    const int base = D == 0 ? c * kPVolS + (a2 * kPY + a1) * kPXs
+                            : (D == 1 ? c * kPVolS + a2 * (kPY * kPXs) + a1 : c * kPVolS + a2 * kPXs + a1);
     const int nb = E.nb[D];
-    for (int t = lane; t < LA * LB; t += 32) {
-        const int a1 = t % LA, a2 = t / LA;
-        const int base = D == 0 ? (a2 * kPY + a1) * kPX : (D == 1 ? a2 * (kPY * kPX) + a1 : a2 * kPX + a1);
-        float u[4], v[4];
-        int loc[4];
+    float u[4], v[4];
+    int loc[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int l = a < nb ? E.id[D][a] - o : -1;
-            loc[a] = (l >= 0 && l < ext) ? l : -1;
-            u[a] = loc[a] >= 0 ? P[base + loc[a] * stride] : 0.f;
-        }
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            float acc = 0.f;
-#pragma unroll
-            for (int a = 0; a < 4; ++a) acc = fmaf(E.e[D][a][b], u[a], acc);
-            v[b] = acc;
-        }
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-            if (loc[b] >= 0) P[base + loc[b] * stride] = v[b];
+    for (int a = 0; a < 4; ++a) {
+        const int l = a < nb ? E.id[D][a] - o : -1;
+        loc[a] = (l >= 0 && l < ext) ? l : -1;
+        u[a] = loc[a] >= 0 ? P[base + loc[a] * stride] : 0.f;
     }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        float acc = 0.f;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc = fmaf(E.e[D][a][b], u[a], acc);
+        v[b] = acc;
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        if (loc[b] >= 0) P[base + loc[b] * stride] = v[b];
 }
 
 // W <- E W on the boundary control points of direction D of a brick's node partials P (patch
@@ -271,7 +289,7 @@ __device__ __forceinline__ float row_scale(const TcInst &I, const BrickBox &bb, 
     return 0.f;
 }
 
-// 25 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
+// 26 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
 // the compiler caps a thread at 72
 __global__ void __launch_bounds__(kPtThreads, 1)
 apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const BrickDesc *__restrict__ desc,
@@ -279,10 +297,10 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     extern __shared__ __align__(1024) float psm[];
     float *sB = psm;                      // [hi, lo][kBFl]
     float *sAlo = psm + 2 * kBFl;         // [2 slots][kAloFl] A_lo operand
-    float *sP = sAlo + 2 * kAloFl;        // [3][kPatBuf] input patches, each builder warp its own part
-    float *sZb = sP + 3 * kPatBuf;        // [2][kZFl] per-layer node partials, by brick parity
+    float *sP = sAlo + 2 * kAloFl;        // [kNPatch][kPatBuf] input patches
+    float *sZb = sP + kNPatch * kPatBuf;  // [2][kZFl] per-layer node partials, by brick parity
     float *sW = sZb + 2 * kZFl;           // [3 * kPVol] node partials of a boundary brick (E applied)
-    __shared__ __align__(8) uint64_t bars[10];
+    __shared__ __align__(8) uint64_t bars[10 + 3 * kNPatch];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
     // this CTA's bricks of systems whose solve goes on: bricks blockIdx.x + k gridDim.x in order
@@ -291,7 +309,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     __shared__ int s_nlist;
     __shared__ unsigned s_act[kMaxInst / 32];   // bit i: system i's solve goes on
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
-             *fin = bars + 9;
+             *fin = bars + 9, *p_full = bars + 10, *p_empty = bars + 10 + kNPatch, *t_full = bars + 10 + 2 * kNPatch;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     {
         // stream compaction, kPtThreads candidates per round: each warp ballots its 32, the counts
@@ -346,6 +364,11 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         tc::mbar_init(&d_empty[1], kRoleThreads);
         tc::mbar_init(b_full, 1);
         tc::mbar_init(fin, 1);
+        for (int b = 0; b < kNPatch; ++b) {
+            tc::mbar_init(&p_full[b], 32);
+            tc::mbar_init(&p_empty[b], kRoleThreads);
+            tc::mbar_init(&t_full[b], 1);
+        }
         tc::fence_mbar_init();
         s_abort = 0;
     }
@@ -356,105 +379,35 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
 
     if (warp < kRoleWarps) {
         // ------------------------------ builders ------------------------------
-        // warp = 4 c + q: component c of the 32 elements of z-layer q (TMEM lanes 32 q ..).  Each
-        // warp fetches and transforms its own patch (component c, z-rows q .. q + 2: exactly the
-        // control points of its elements), so the builders never wait for each other.
+        // warp = 4 c + q: component c of the 32 elements of z-layer q (TMEM lanes 32 q ..); the
+        // builders wait only for their patch buffer and their A slot, never for each other.
         const int c = warp >> 2, q = warp & 3;
         const int lx = lane & 7, ly = lane >> 3;
         const unsigned FULLW = 0xffffffffu;
-        // lane l < 18 copies row l = (pz, py) of kPX floats, in 8-byte pieces when the row is whole
-        // and starts on an even float (always when the x control-point count is even), else float
-        // by float
-        auto load_patch = [&](int k, const BrickDesc &d, float *dst) {
-            if (k < nmine && lane < 3 * kPY) {
-                const TcInst &I = insts[d.inst];
-                const Geom &g = I.g;
-                const BrickBox bb = desc_box(d);
-                const int py = lane % kPY, pz = lane / kPY;
-                const int gy = bb.y0 + py, gz = bb.z0 + q + pz;
-                float *drow = dst + lane * kPX;
-                if (gy < g.cy && gz < g.cz) {
-                    const long long off = (long long)c * g.nsc + ((long long)gz * g.cy + gy) * g.cx + bb.x0;
-                    const float *srow = I.xin + off;
-                    if (bb.x0 + kPX <= g.cx && !(off & 1)) {
-#pragma unroll
-                        for (int px = 0; px < kPX; px += 2) tc::cp_async8(drow + px, srow + px);
-                    } else {
-#pragma unroll
-                        for (int px = 0; px < kPX; ++px) {
-                            if (bb.x0 + px < g.cx) tc::cp_async4(drow + px, srow + px);
-                            else drow[px] = 0.f;
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int px = 0; px < kPX; ++px) drow[px] = 0.f;
-                }
-            }
-            tc::cp_async_commit();
-        };
-        float *sPw = sP + warp * kWPat;   // this warp's part of each patch buffer
-        // three patch buffers: the brick two ahead is fetched while one is built; descriptors are
-        // read three bricks ahead (d1, d2, d3 = bricks it + 1, it + 2, it + 3)
-        auto get_desc = [&](int k) {
-            BrickDesc d{};
-            if (k < nmine) d = desc[s_list[k]];
-            return d;
-        };
-        const BrickDesc d0 = get_desc(0);
-        BrickDesc d1 = get_desc(1), d2 = get_desc(2), d3 = get_desc(3);
-        load_patch(0, d0, sPw);
-        load_patch(1, d1, sPw + kPatBuf);
         const int r = q * 32 + lane;
-        BrickDesc dcur = d0;
-        unsigned fl_next = desc_flags(d0);
-        float se_next = row_scale(insts[d0.inst], desc_box(d0), r);
+        // s_e of this thread's element is read one brick ahead, descriptors two
+        BrickDesc dn = desc[s_list[0]];
+        BrickDesc d1 = nmine > 1 ? desc[s_list[1]] : BrickDesc{};
+        float se_next = row_scale(insts[dn.inst], desc_box(dn), r);
         for (int it = 0; it < nmine; ++it) {
-            const int s = it & 1, pb = it % 3;
-            const unsigned fl = fl_next;   // bit d: the brick's patch holds boundary points of d
+            const int s = it & 1, pb = it % kNPatch;
             const float se = se_next;      // s_e k of this thread's element (0 outside the grid)
-            const BrickDesc d = dcur;
-            const TcInst &I = insts[d.inst];
-            const Geom &g = I.g;
-            const BrickBox bb = desc_box(d);
-            if (it + 1 < nmine) {
-                fl_next = desc_flags(d1);
-                se_next = row_scale(insts[d1.inst], desc_box(d1), r);
-            }
-            load_patch(it + 2, d2, sPw + ((it + 2) % 3) * kPatBuf);
-            dcur = d1;
-            d1 = d2;
-            d2 = d3;
-            d3 = get_desc(it + 4);
+            const BrickBox bb = desc_box(dn);
+            if (it + 1 < nmine) se_next = row_scale(insts[d1.inst], desc_box(d1), r);
+            dn = d1;
+            d1 = it + 2 < nmine ? desc[s_list[it + 2]] : BrickDesc{};
             const bool valid = lx < bb.ex_n && ly < bb.ey_n && q < bb.ez_n;
             const float vm = valid ? se : 0.f;
-            tc::cp_async_wait<2>();
-            const bool ok = it < 2 || pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err);
+            const bool ok = pt_wait(&p_full[pb], uint32_t(it / kNPatch) & 1u, &s_abort, err) &&
+                            (it < 2 || pt_wait(&a_empty[s], uint32_t((it >> 1) - 1) & 1u, &s_abort, err));
             // the warp leaves together on abort (nothing of the other warps waits for it here)
             if (!__all_sync(FULLW, ok && s_abort == 0)) break;
-            __syncwarp();   // every lane's rows of this brick have landed
-            float *Pw = sPw + pb * kPatBuf;
-            if (fl) {   // V = E' u on the boundary control planes, one direction after the other
-                const Edge &E = *I.edge;
-                if (fl & 1u) {
-                    edge_in_warp<0>(Pw, E, bb.x0, min(kPX, g.cx - bb.x0), lane);
-                    __syncwarp();
-                }
-                if (fl & 2u) {
-                    edge_in_warp<1>(Pw, E, bb.y0, min(kPY, g.cy - bb.y0), lane);
-                    __syncwarp();
-                }
-                if (fl & 4u) {
-                    edge_in_warp<2>(Pw, E, bb.z0 + q, min(3, g.cz - bb.z0 - q), lane);
-                    __syncwarp();
-                }
-            }
             tc::fence_after_sync();
-            const float *Pc = Pw + ly * kPX + lx;
+            const float *Pc = sP + pb * kPatBuf + c * kPVolS + q * (kPY * kPXs) + ly * kPXs + lx;
             float v[27];
 #pragma unroll
-            for (int a = 0; a < 27; ++a) v[a] = Pc[(a / 9) * (kPY * kPX) + ((a / 3) % 3) * kPX + a % 3];
-        // Element-local shift: K_u maps a constant per-component field to zero, so subtracting
+            for (int a = 0; a < 27; ++a) v[a] = Pc[(a / 9) * (kPY * kPXs) + ((a / 3) % 3) * kPXs + a % 3];
+            // Element-local shift: K_u maps a constant per-component field to zero, so subtracting
             // the element's centre control value changes nothing in exact arithmetic while the
             // split operands carry only the variation across the element; the TF32 splitting
             // error then scales with that variation instead of with |u| (smooth, low-energy
@@ -462,6 +415,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             const float nctr = -v[13] * vm;
 #pragma unroll
             for (int a = 0; a < 27; ++a) v[a] = fmaf(v[a], vm, nctr);   // s_e (v - ctr), or 0 outside the grid
+            tc::mbar_arrive(&p_empty[pb]);   // this thread's reads of the patch are done
             // A_hi into TMEM (lane = element), A_lo into shared memory in the canonical layout
             const uint32_t col = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(s * kColSlot + c * 32);
             float *alo = sAlo + s * kAloFl + canon(q * 32 + lane, c * 32, kTcM);
@@ -479,9 +433,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(&a_full[s]);
-            __syncwarp();   // the warp is done with this patch before it is refilled
         }
-        tc::cp_async_wait<0>();
     } else if (warp < 2 * kRoleWarps) {
         // ------------------------------ epilogue ------------------------------
         // warp = 12 + 4 c + q: component c of z-layer q; lane = lx + 8 ly = element (lx, ly, q)
@@ -605,6 +557,65 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             for (int k = 0; k < 3; ++k)
                 if (et + k * kRoleThreads < 3 * kPVol) ob[k * kRoleThreads] = sums[k];
         }
+    } else if (warp == kLoaderWarp) {
+        // ------------------------------ loader ------------------------------
+        // brick k goes to buffer k % kNPatch once the builders have read brick k - kNPatch from
+        // it; kLoadAhead bricks later the warp waits for its copy, runs the boundary transform and
+        // every lane arrives on the buffer's p_full (its own writes are done).
+        const unsigned FULLW = 0xffffffffu;
+        int issued = 0, landed = 0, last_inst = -1;
+        for (int k = 0; k < nmine + kLoadAhead; ++k) {
+            if (k < nmine) {
+                const int b = k % kNPatch;
+                const bool ok = k < kNPatch || pt_wait(&p_empty[b], uint32_t(k / kNPatch - 1) & 1u, &s_abort, err);
+                if (!__all_sync(FULLW, ok && s_abort == 0)) break;
+                if (lane == 0) {
+                    const BrickDesc d = desc[s_list[k]];
+                    const BrickBox bb = desc_box(d);
+                    const CUtensorMap *tm = &insts[d.inst].tmap;
+                    if ((int)d.inst != last_inst) {
+                        tc::fence_tensormap_acquire(tm);
+                        last_inst = (int)d.inst;
+                    }
+                    tc::fence_proxy_async();   // earlier generic accesses of the buffer before the copy
+                    tc::mbar_arrive_expect_tx(&t_full[b], kPatchBytes);
+                    tc::tma_load_4d(sP + b * kPatBuf, tm, bb.x0, bb.y0, bb.z0, 0, &t_full[b]);
+                }
+                issued = k + 1;
+            }
+            const int j = k - kLoadAhead;
+            if (j >= 0) {
+                const int b = j % kNPatch;
+                const bool ok = pt_wait(&t_full[b], uint32_t(j / kNPatch) & 1u, &s_abort, err);
+                if (!__all_sync(FULLW, ok && s_abort == 0)) break;
+                landed = j + 1;
+                const BrickDesc d = desc[s_list[j]];
+                const unsigned fl = desc_flags(d);
+                float *P = sP + b * kPatBuf;
+                if (fl) {   // V = E' u on the boundary control planes, one direction after the other
+                    const TcInst &I = insts[d.inst];
+                    const Geom &g = I.g;
+                    const Edge &E = *I.edge;
+                    const BrickBox bb = desc_box(d);
+                    if (fl & 1u) {
+                        for (int t = lane; t < 3 * kPY * kPZ; t += 32) edge_in<0>(P, E, bb.x0, min(kPX, g.cx - bb.x0), t);
+                        __syncwarp();
+                    }
+                    if (fl & 2u) {
+                        for (int t = lane; t < 3 * kPX * kPZ; t += 32) edge_in<1>(P, E, bb.y0, min(kPY, g.cy - bb.y0), t);
+                        __syncwarp();
+                    }
+                    if (fl & 4u) {
+                        for (int t = lane; t < 3 * kPX * kPY; t += 32) edge_in<2>(P, E, bb.z0, min(kPZ, g.cz - bb.z0), t);
+                        __syncwarp();
+                    }
+                }
+                tc::mbar_arrive(&p_full[b]);
+            }
+        }
+        // after an abort: copies still in flight land before the CTA ends
+        for (int j = landed; j < issued; ++j)
+            tc::mbar_wait_bounded(&t_full[j % kNPatch], uint32_t(j / kNPatch) & 1u, kWaitLimit);
     } else if (lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
         constexpr uint32_t idesc = tc::idesc_tf32(kTcM, kTcN);
@@ -778,9 +789,10 @@ __device__ __forceinline__ void block_sum5(double (&v)[5]) {
 //   which give the convergence test and beta = r_new'z_new / r'z.  When the FP32 residual has
 //   gained the replacement factor (or the segment is long) the state asks the host for an FP64
 //   residual replacement instead.
-//   Phase B: x += alpha p, r -= alpha Ap, p = D^-1 r + beta p (when the iteration goes on), and the
-//   exact r'r and r'z of the new r as per-CTA partials, which the next launch reduces in place of
-//   the formulas (so they bridge one iteration only).
+//   Phase B: x += alpha p, r -= alpha Ap, p = D^-1 r + beta p (when the iteration goes on) with
+//   the next apply's input pin (p with the fixed DOFs zeroed, rows padded), and the exact r'r and
+//   r'z of the new r as per-CTA partials, which the next launch reduces in place of the formulas
+//   (so they bridge one iteration only).
 // The system's first CTA writes its state.  All CTAs of a system take the same branches; the CTAs
 // of a stopped system only arrive at the barrier.
 __global__ void __launch_bounds__(kTailThreads, 4)
@@ -808,7 +820,7 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
     float *__restrict__ x = I.x;
     float *__restrict__ r = I.r;
     float *__restrict__ p = I.p;
-    float *__restrict__ pm = I.pm;
+    float *__restrict__ pin = I.pin;
     float *__restrict__ ap = I.ap;
     double *pa = I.part, *pb = I.part + 5 * G;   // phase A partials [5][G], exact r'r, r'z [2][G]
     // exact r'r and r'z of the current r: from the state after an initialisation or replacement,
@@ -923,6 +935,10 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
     // B. x += alpha p, r -= alpha Ap; the direction only when the iteration goes on
     const float alpha = float(s_ab[0]), beta = float(s_ab[1]);
     const bool go = s_stat == 0;
+    const bool ident = mask_mode == ICC_MASK_IDENTITY;
+    // index of i in the padded layout: i + (i / cx) (cxp - cx), the quotient kept up to date
+    const long long pad = I.cxp - g.cx, Tq = T / g.cx, Tr = T % g.cx;
+    long long row = t0 / g.cx, col = t0 % g.cx;
     double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for (long long i = t0; i < n; i += T) {
         const float pi = p[i];
@@ -934,12 +950,15 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
         v[1] += double(ri) * double(zi);
         if (go) {
             const float w = zi + beta * pi;
-            if (pm) {
-                p[i] = w;
-                pm[i] = mask[i] ? w : 0.f;
-            } else {
-                p[i] = (mask && !mask[i]) ? 0.f : w;
-            }
+            const float wm = (mask && !mask[i]) ? 0.f : w;
+            p[i] = ident ? w : wm;
+            pin[i + row * pad] = wm;
+        }
+        row += Tq;
+        col += Tr;
+        if (col >= g.cx) {
+            col -= g.cx;
+            ++row;
         }
     }
     block_sum5(v);
@@ -1154,13 +1173,43 @@ static int setup_edge(const Op &op, Edge &edge, std::vector<double> &kunif) {
     return ICC_OK;
 }
 
+// The tensor map of a system's apply input: dimensions (cx, cy, cz, 3) with row pitch cxp, boxes of
+// 12 x 6 x 6 x 3 floats (one brick's patch), zero fill outside the grid.  The driver's encoder is
+// looked up through the runtime, so the library needs no link to the driver library.
+static int encode_input_map(const Op &op, VecSet &v) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return set_error(ICC_CUDA_ERROR, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[4] = {(cuuint64_t)op.g.cx, (cuuint64_t)op.g.cy, (cuuint64_t)op.g.cz, 3};
+    const cuuint64_t strides[3] = {(cuuint64_t)v.cxp * 4, (cuuint64_t)v.cxp * op.g.cy * 4,
+                                   (cuuint64_t)v.cxp * op.g.cy * op.g.cz * 4};
+    const cuuint32_t box[4] = {kPXs, kPY, kPZ, 3};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = encode(&v.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, v.pin32, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ICC_CUDA_ERROR, "tensor map of the apply input: error " + std::to_string((int)r));
+    return ICC_OK;
+}
+
 static int vecset_alloc(const Op &op, VecSet &v, int part_cap) {
     const size_t n = (size_t)op.ndof;
     int rc;
     if ((rc = dalloc(&v.patch32, (size_t)op.g.nbricks * 3 * kPVol, "alloc mixed"))) return rc;
-    float **f32[] = {&v.rhs32, &v.x32, &v.r32, &v.p32, &v.ap32, &v.xm32, &v.inv32};
+    float **f32[] = {&v.rhs32, &v.x32, &v.r32, &v.p32, &v.ap32, &v.inv32};
     for (float **p : f32)
         if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
+    v.cxp = (op.g.cx + 3) & ~3;
+    const size_t npad = (size_t)3 * v.cxp * op.g.cy * op.g.cz;
+    if ((rc = dalloc(&v.pin32, npad, "alloc mixed"))) return rc;
+    ICC_CUDA(cudaMemset(v.pin32, 0, npad * sizeof(float)), "clear apply input");
+    if ((rc = encode_input_map(op, v))) return rc;
     double **f64[] = {&v.x64, &v.r64, &v.y64};
     for (double **p : f64)
         if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
@@ -1170,7 +1219,7 @@ static int vecset_alloc(const Op &op, VecSet &v, int part_cap) {
 }
 
 static void vecset_free(VecSet &v) {
-    void *bufs[] = {v.patch32, v.rhs32, v.x32, v.r32, v.p32, v.ap32, v.xm32, v.inv32, v.x64, v.r64, v.y64, v.part};
+    void *bufs[] = {v.patch32, v.rhs32, v.x32, v.r32, v.p32, v.ap32, v.inv32, v.pin32, v.x64, v.r64, v.y64, v.part};
     for (void *p : bufs)
         if (p) cudaFree(p);
     v = VecSet();
@@ -1298,23 +1347,34 @@ int mixed_on_scale_update(Op &op) {
 }
 
 // xm = mask .* x (the brick apply reads its input unmasked)
-__global__ void mask_copy_kernel(long long n, const float *__restrict__ x, const uint8_t *__restrict__ mask,
-                                 float *__restrict__ xm) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        xm[i] = mask[i] ? x[i] : 0.f;
+// pin = x with the fixed DOFs zeroed (mask given), rows of cx values stored with pitch cxp; one
+// warp per row of control points
+__global__ void pad_input_kernel(long long rows, int cx, int cxp, const float *__restrict__ x,
+                                 const uint8_t *__restrict__ mask, float *__restrict__ pin) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long rw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; rw < rows; rw += warps)
+        for (int ix = lane; ix < cx; ix += 32) {
+            const long long i = rw * cx + ix;
+            pin[rw * cxp + ix] = (mask && !mask[i]) ? 0.f : x[i];
+        }
 }
 
-// The instance entry of system (op, v) with PCG state st (null: a plain apply of xin).
-static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, const float *xin, int cta0, int ncta, float kfac) {
+static void enqueue_pad_input(const Op &op, const VecSet &v, const float *x, cudaStream_t s) {
+    const uint8_t *mask = op.mask_mode != ICC_MASK_NONE ? op.d_mask : nullptr;
+    pad_input_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(3LL * op.g.cy * op.g.cz, op.g.cx, v.cxp, x, mask, v.pin32);
+}
+
+// The instance entry of system (op, v) with PCG state st (null: a plain apply of v.pin32).
+static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, int cta0, int ncta, float kfac) {
     const MixedState &ms = *op.mixed;
-    const bool ident = op.mask_mode == ICC_MASK_IDENTITY;
     TcInst I;
     std::memset(&I, 0, sizeof(I));
     I.g = op.g;
     I.cta0 = cta0;
     I.ncta = ncta;
     I.kfac = kfac;
-    I.xin = xin ? xin : (ident ? v.xm32 : v.p32);
+    I.tmap = v.tmap;
     I.scale = ms.d_scale32;
     I.edge = ms.d_edge;
     I.patch = v.patch32;
@@ -1325,7 +1385,8 @@ static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, const float
     I.x = v.x32;
     I.r = v.r32;
     I.p = v.p32;
-    I.pm = ident ? v.xm32 : nullptr;
+    I.pin = v.pin32;
+    I.cxp = v.cxp;
     I.ap = v.ap32;
     I.part = v.part;
     I.st = st;
@@ -1353,16 +1414,12 @@ static cudaError_t launch_tail(cudaStream_t s, const TcInst *d_insts, int ninst,
     return cudaLaunchKernelEx(&cfg, pcg_tail_kernel, d_insts, ninst, ctr, err, limit);
 }
 
-// enqueue y32 = A x32 with the tensor-core apply; a masked operator first zeroes the fixed DOFs of
-// the input (into the xm32 scratch vector), the node-side pass applies the output rule
+// enqueue y32 = A x32 with the tensor-core apply: the input goes to the padded apply input (fixed
+// DOFs of a masked operator zeroed), the node-side pass applies the output rule
 static int enqueue_apply_tc(Op &op, const float *x, float *y) {
     MixedState &ms = *op.mixed;
-    const float *xin = x;
-    if (op.mask_mode != ICC_MASK_NONE) {
-        mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.ndof, x, op.d_mask, ms.v.xm32);
-        xin = ms.v.xm32;
-    }
-    const TcInst I = make_inst(op, ms.v, nullptr, xin, 0, 0, 1.f);
+    enqueue_pad_input(op, ms.v, x, op.stream);
+    const TcInst I = make_inst(op, ms.v, nullptr, 0, 0, 1.f);
     ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
     launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms);
     gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
@@ -1419,7 +1476,8 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     if (rc) return rc;
     MixedState &ms = *op.mixed;
     if ((rc = clear_flags(op.stream, ms.d_err, ms.d_grid_ctr))) return rc;
-    const TcInst I = make_inst(op, ms.v, nullptr, x, 0, 0, 1.f);
+    enqueue_pad_input(op, ms.v, x, op.stream);
+    const TcInst I = make_inst(op, ms.v, nullptr, 0, 0, 1.f);
     ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
     std::vector<cudaEvent_t> ev(3 * size_t(reps));
     for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
@@ -1624,10 +1682,8 @@ static int init_items(MixedBatch &bt, std::vector<MixedItem> &items, double delt
                                                     trial ? (1LL << 40) : (long long)it.max_iter);
         ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, 1.0, trial ? 0.0 : delta, kMaxSegment, check_every);
         launches += 4;
-        if (op.mask_mode == ICC_MASK_IDENTITY) {
-            mask_copy_kernel<<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.p32, op.d_mask, v.xm32);
-            launches++;
-        }
+        enqueue_pad_input(op, v, v.p32, s);
+        launches++;
     }
     ICC_CUDA(cudaGetLastError(), "mixed init");
     return ICC_OK;
@@ -1721,11 +1777,10 @@ static int run_mixed(MixedBatch &bt, std::vector<MixedItem> &items, const icc_so
             ru_replace_finalize<<<1, kVecThreads, 0, s>>>(op.d_partials, op.vec_blocks, bt.d_state + i);
             ru_arm_kernel<<<1, 1, 0, s>>>(bt.d_state + i, it.res, delta, kMaxSegment, check_every);
             // the direction update of this iteration, with the replaced residual
-            const bool ident = op.mask_mode == ICC_MASK_IDENTITY;
             pcg_p_kernel<float><<<op.vec_blocks, kVecThreads, 0, s>>>(op.ndof, v.r32, v.inv32, v.p32, bt.d_state + i,
-                                                                      op.mask_mode != ICC_MASK_NONE ? op.d_mask : nullptr,
-                                                                      ident ? v.xm32 : nullptr);
-            launches += 4;
+                                                                      op.mask_mode == ICC_MASK_ZERO ? op.d_mask : nullptr);
+            enqueue_pad_input(op, v, v.p32, s);
+            launches += 5;
         }
         ICC_CUDA(cudaGetLastError(), "replacement");
     }
@@ -1796,7 +1851,7 @@ int mixed_solve(Op &op, const double *b, const double *diag, double tol, int64_t
     bt.limit = ms.grid_wait_limit;
     bt.graph = ms.graph;
     if (!ms.graph || ms.graph_batch != check_every || ms.graph_limit != ms.grid_wait_limit) {
-        const TcInst I = make_inst(op, ms.v, ms.d_state, nullptr, 0, bt.tail_grid, 1.f);
+        const TcInst I = make_inst(op, ms.v, ms.d_state, 0, bt.tail_grid, 1.f);
         ICC_CUDA(cudaMemcpyAsync(bt.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
         bt.graph = ms.graph;
         if ((rc = capture_graph(bt, check_every))) return rc;
@@ -1885,7 +1940,7 @@ static int upload_table(MixedBatch &bt, std::vector<MixedItem> &items, const std
     int cta = 0;
     for (size_t i = 0; i < items.size(); ++i) {
         if (items[i].v->part_cap < ncta[i]) return set_error(ICC_BAD_ARG, "batched mixed solve: partial buffer too small");
-        tab[i] = make_inst(*items[i].op, *items[i].v, bt.d_state + i, nullptr, cta, ncta[i], items[i].kfac);
+        tab[i] = make_inst(*items[i].op, *items[i].v, bt.d_state + i, cta, ncta[i], items[i].kfac);
         cta += ncta[i];
     }
     bt.tail_grid = cta;

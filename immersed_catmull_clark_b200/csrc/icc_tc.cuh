@@ -175,6 +175,23 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
 }
 
 // 4-byte asynchronous global -> shared copy (LDGSTS) and its group fences
+// Tiled TMA load of a 4-D box (coordinates x fastest) into shared memory, completing on `bar`
+// (transaction bytes); no multicast.
+__device__ __forceinline__ void tma_load_4d(void *dst_smem, const void *tmap, int x, int y, int z, int w,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(smem_addr(dst_smem)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(w),
+        "r"(smem_addr(bar))
+        : "memory");
+}
+
+// A tensor map written to global memory by the host: acquire it for the async proxy before use.
+__device__ __forceinline__ void fence_tensormap_acquire(const void *tmap) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(tmap))
+                 : "memory");
+}
+
 __device__ __forceinline__ void cp_async4(void *dst_smem, const void *src_gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst_smem)), "l"(src_gmem) : "memory");
 }
