@@ -138,10 +138,11 @@ struct MixedState {
 // One CTA per SM walks the bricks blockIdx.x, blockIdx.x + gridDim.x, ... of the batch's brick
 // numbering (all bricks of all systems), skipping systems whose solve has stopped.  Roles
 // (26 warps):
-//   warp 25 (loader): one thread fetches the input patch of each brick (3 x 6 x 6 x 12 control
-//     values, zero outside the grid) with one TMA copy, up to three bricks ahead, into one of four
-//     patch buffers; the warp transforms the patches of bricks at the grid's ends by E' (the
-//     boundary extraction) and hands each buffer to the builders through an mbarrier;
+//   warps 25-27 (loaders): one thread fetches the input patch of each brick (3 x 6 x 6 x 12
+//     control values, zero outside the grid) with one TMA copy, up to four bricks ahead, into one
+//     of five patch buffers; warp 25 + c transforms component c of the patches of bricks at the
+//     grid's ends by E' (the boundary extraction), and the three warps hand each buffer to the
+//     builders through an mbarrier;
 //   warps 0-11 (builders, warp 4 c + q: component c of z-layer q): gather each element's 27
 //     values of component c from the shared patch, shift them by the element's centre value and
 //     scale by s_e, split into TF32 hi/lo and store A_hi into TMEM (row m = element m = lane m)
@@ -160,10 +161,10 @@ struct MixedState {
 // the flag over the role, so all threads of a role leave their loop at the same brick; the MMA
 // thread stops issuing, then commits once more and waits (bounded) for that commit, so no MMA
 // of the CTA is in flight when TMEM is released.  The host reports ICC_TIMEOUT.
-constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24, loader: 25
+constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24, loaders: 25-27
 constexpr int kRoleThreads = kRoleWarps * 32;
 constexpr int kMmaWarp = 2 * kRoleWarps, kLoaderWarp = 2 * kRoleWarps + 1;
-constexpr int kPtThreads = (2 * kRoleWarps + 2) * 32;
+constexpr int kPtThreads = (2 * kRoleWarps + 4) * 32;
 constexpr int kColSlot = kTcK;         // A_hi slot s: TMEM columns s*96 + [0,96)
 constexpr int kColD = 2 * kColSlot;    // accumulator buffer d: TMEM columns 192 + d*96 + [0,96)
 constexpr int kAloFl = kTcM * kTcK;    // A_lo slot (shared memory, canonical K-major): floats
@@ -174,10 +175,10 @@ constexpr int kPXs = 12;                        // x extent of an input patch ro
 constexpr int kPVolS = kPZ * kPY * kPXs;        // per component
 constexpr uint32_t kPatchBytes = 3 * kPVolS * 4;   // one TMA box: 5,184 B
 constexpr int kPatBuf = 1312;                   // floats per patch buffer (5,248 B: 128-byte aligned)
-constexpr int kNPatch = 4;                      // patch buffers (the loader runs up to 3 bricks ahead)
-constexpr int kLoadAhead = 2;                   // bricks whose copies are in flight while one is finished
+constexpr int kNPatch = 5;                      // patch buffers (the loaders run up to 4 bricks ahead)
+constexpr int kLoadAhead = 3;                   // bricks whose copies are in flight while one is finished
 static_assert(kPatBuf * 4 >= (int)kPatchBytes && (kPatBuf * 4) % 128 == 0, "patch buffer");
-constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + kNPatch * kPatBuf + 2 * kZFl + 3 * kPVol) * 4;  // 214,624 B
+constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + kNPatch * kPatBuf + 2 * kZFl + 3 * kPVol) * 4;  // 219,872 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
 // Each test may sleep up to kWaitSleepNs; with kWaitLimit tests a wait gives up after at most
@@ -289,7 +290,7 @@ __device__ __forceinline__ float row_scale(const TcInst &I, const BrickBox &bb, 
     return 0.f;
 }
 
-// 26 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
+// 28 warps: registers are split over the 4 SM sub-partitions, so 7 warps share 16,384 of them and
 // the compiler caps a thread at 72
 __global__ void __launch_bounds__(kPtThreads, 1)
 apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const BrickDesc *__restrict__ desc,
@@ -365,7 +366,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         tc::mbar_init(b_full, 1);
         tc::mbar_init(fin, 1);
         for (int b = 0; b < kNPatch; ++b) {
-            tc::mbar_init(&p_full[b], 32);
+            tc::mbar_init(&p_full[b], 96);
             tc::mbar_init(&p_empty[b], kRoleThreads);
             tc::mbar_init(&t_full[b], 1);
         }
@@ -445,8 +446,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         const uint32_t dcol0 = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(kColD + c * 32);
         const unsigned FULL = 0xffffffffu;
         // lane masks of the node sums as multipliers (FMA instead of selects)
-        const float mx1 = lx >= 1 ? 1.f : 0.f, mx2 = lx >= 2 ? 1.f : 0.f;
-        const float my1 = ly >= 1 ? 1.f : 0.f, my2 = ly >= 2 ? 1.f : 0.f;
+        const float mx1 = lx >= 1 ? 1.f : 0.f, my1 = ly >= 1 ? 1.f : 0.f;
         // z-sum: this thread's outputs i = et + k * 384 of the brick; the term of layer lz = pz - az
         // sits at sZ[((lz * 3 + az) * 3 + ci) * 60 + pyx] = sZ[zb - 360 az] with zb = 540 pz + 60 ci + pyx
         int zb[3], zpz[3];
@@ -474,30 +474,26 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             float res[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
-            // x, in place: node px = lx gets v[ax=0](lx) + v[1](lx-1) + v[2](lx-2) in res[o]; lanes
-            // lx = 7 also carry px = 8 (v[1](7) + v[2](6)) in res[o+1] and px = 9 (v[2](7)) in res[o+2]
+            // x, in place: t(lx) = v[ax=1](lx) + v[2](lx-1), then node px = lx gets v[0](lx) + t(lx-1) in
+            // res[o]; lanes lx = 7 also carry px = 8 (t(7)) in res[o+1] and px = 9 (v[2](7)) in res[o+2]
 #pragma unroll
             for (int az = 0; az < 3; ++az)
 #pragma unroll
                 for (int ay = 0; ay < 3; ++ay) {
                     const int o = 3 * ay + 9 * az;
-                    const float a0 = res[o], a1 = res[o + 1], a2 = res[o + 2];
-                    const float u1 = __shfl_up_sync(FULL, a1, 1), u2 = __shfl_up_sync(FULL, a2, 2);
-                    const float w1 = __shfl_up_sync(FULL, a2, 1);
-                    res[o] = fmaf(mx2, u2, fmaf(mx1, u1, a0));   // (a0 + u1) + u2 on lanes that have them
-                    res[o + 1] = fmaf(mx1, w1, a1);
+                    const float t = fmaf(mx1, __shfl_up_sync(FULL, res[o + 2], 1), res[o + 1]);
+                    res[o] = fmaf(mx1, __shfl_up_sync(FULL, t, 1), res[o]);
+                    res[o + 1] = t;
                 }
-            // y: node py = ly gets X[ay=0](ly) + X[1](ly-1) + X[2](ly-2); lanes ly = 3 also carry
-            // py = 4 and py = 5.  Results are this layer's partials for z-offset az.
+            // y, the same along ly (lanes 8 apart): node py = ly gets X[ay=0](ly) + (X[1] + X[2](. - 1))(ly - 1);
+            // lanes ly = 3 also carry py = 4 and py = 5.  Results are this layer's partials for z-offset az.
 #pragma unroll
             for (int az = 0; az < 3; ++az)
 #pragma unroll
                 for (int var = 0; var < 3; ++var) {
                     const float a0 = res[9 * az + var], a1 = res[9 * az + 3 + var], a2 = res[9 * az + 6 + var];
-                    const float s1 = __shfl_up_sync(FULL, a1, 8), s2 = __shfl_up_sync(FULL, a2, 16);
-                    const float t1 = __shfl_up_sync(FULL, a2, 8);
-                    const float yv = fmaf(my2, s2, fmaf(my1, s1, a0));
-                    const float y4 = fmaf(my1, t1, a1);
+                    const float y4 = fmaf(my1, __shfl_up_sync(FULL, a2, 8), a1);
+                    const float yv = fmaf(my1, __shfl_up_sync(FULL, y4, 8), a0);
                     const int px = var == 0 ? lx : 7 + var;
                     if (var == 0 || lx == 7) {
                         float *zp = sZ + (((q * 3 + az) * 3 + c) * kPY) * kPX + px;
@@ -557,15 +553,18 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             for (int k = 0; k < 3; ++k)
                 if (et + k * kRoleThreads < 3 * kPVol) ob[k * kRoleThreads] = sums[k];
         }
-    } else if (warp == kLoaderWarp) {
-        // ------------------------------ loader ------------------------------
+    } else if (warp >= kLoaderWarp) {
+        // ------------------------------ loaders ------------------------------
         // brick k goes to buffer k % kNPatch once the builders have read brick k - kNPatch from
-        // it; kLoadAhead bricks later the warp waits for its copy, runs the boundary transform and
-        // every lane arrives on the buffer's p_full (its own writes are done).
+        // it (warp 25 issues the copy); kLoadAhead bricks later each loader warp waits for the
+        // copy, transforms its component and its lanes arrive on the buffer's p_full (their own
+        // writes are done).  Every loader warp waits for each copy once, in brick order, so no
+        // wait runs a phase ahead of its barrier.
         const unsigned FULLW = 0xffffffffu;
+        const int lc = warp - kLoaderWarp;
         int issued = 0, landed = 0, last_inst = -1;
         for (int k = 0; k < nmine + kLoadAhead; ++k) {
-            if (k < nmine) {
+            if (k < nmine && lc == 0) {
                 const int b = k % kNPatch;
                 const bool ok = k < kNPatch || pt_wait(&p_empty[b], uint32_t(k / kNPatch - 1) & 1u, &s_abort, err);
                 if (!__all_sync(FULLW, ok && s_abort == 0)) break;
@@ -598,15 +597,18 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
                     const Edge &E = *I.edge;
                     const BrickBox bb = desc_box(d);
                     if (fl & 1u) {
-                        for (int t = lane; t < 3 * kPY * kPZ; t += 32) edge_in<0>(P, E, bb.x0, min(kPX, g.cx - bb.x0), t);
+                        for (int t = lane; t < kPY * kPZ; t += 32)
+                            edge_in<0>(P, E, bb.x0, min(kPX, g.cx - bb.x0), lc * (kPY * kPZ) + t);
                         __syncwarp();
                     }
                     if (fl & 2u) {
-                        for (int t = lane; t < 3 * kPX * kPZ; t += 32) edge_in<1>(P, E, bb.y0, min(kPY, g.cy - bb.y0), t);
+                        for (int t = lane; t < kPX * kPZ; t += 32)
+                            edge_in<1>(P, E, bb.y0, min(kPY, g.cy - bb.y0), lc * (kPX * kPZ) + t);
                         __syncwarp();
                     }
                     if (fl & 4u) {
-                        for (int t = lane; t < 3 * kPX * kPY; t += 32) edge_in<2>(P, E, bb.z0, min(kPZ, g.cz - bb.z0), t);
+                        for (int t = lane; t < kPX * kPY; t += 32)
+                            edge_in<2>(P, E, bb.z0, min(kPZ, g.cz - bb.z0), lc * (kPX * kPY) + t);
                         __syncwarp();
                     }
                 }
