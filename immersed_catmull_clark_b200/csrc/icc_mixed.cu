@@ -89,7 +89,7 @@ struct TcInst {
     float *x, *r, *p, *ap;
     float *pin;                  // the brick apply's input: the masked p, rows padded to cxp
     int cxp;
-    double *part;                // [7][ncta] partial sums of the fused vector step
+    double *part;                // [9][ncta] partial sums of the fused vector step
     PcgState *st;                // null for a plain apply: every brick is active
 };
 
@@ -103,7 +103,7 @@ struct VecSet {
     int cxp = 0;
     CUtensorMap tmap{};
     double *x64 = nullptr, *r64 = nullptr, *y64 = nullptr;
-    double *part = nullptr;  // [7][tail CTAs]
+    double *part = nullptr;  // [9][tail CTAs]
     int part_cap = 0;
 };
 
@@ -760,19 +760,20 @@ __device__ void grid_arrive(unsigned long long *ctr) {
     }
 }
 
-// Deterministic block reduction of five values at once; the sums are valid in thread 0.
-__device__ __forceinline__ void block_sum5(double (&v)[5]) {
-    __shared__ double ws[5][kTailThreads / 32];
+// Deterministic block reduction of N values at once; the sums are valid in thread 0.
+template <int N>
+__device__ __forceinline__ void block_sum_n(double (&v)[N]) {
+    __shared__ double ws[N][kTailThreads / 32];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) v[k] = warp_sum(v[k]);
+    for (int k = 0; k < N; ++k) v[k] = warp_sum(v[k]);
     __syncthreads();
     if ((threadIdx.x & 31) == 0)
 #pragma unroll
-        for (int k = 0; k < 5; ++k) ws[k][threadIdx.x >> 5] = v[k];
+        for (int k = 0; k < N; ++k) ws[k][threadIdx.x >> 5] = v[k];
     __syncthreads();
     if (threadIdx.x < 32) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < N; ++k) {
             double r = threadIdx.x < (blockDim.x >> 5) ? ws[k][threadIdx.x] : 0.0;
             v[k] = warp_sum(r);
         }
@@ -782,19 +783,24 @@ __device__ __forceinline__ void block_sum5(double (&v)[5]) {
 // One launch for everything of a PCG iteration after the operator (rust/src/solver.rs:38-71),
 // with one grid-wide barrier, for every system of the batch: system i is served by CTAs
 // [cta0, cta0 + ncta) and reduces its own partials.
-//   Phase A, node by node: Ap = the node sum of the brick partials plus the sparse term, output rule applied; and five dot products p'Ap, z'Ap, Ap'D^-1 Ap, r'Ap,
-//   Ap'Ap (z = D^-1 r).
-//   Barrier.  Every CTA of the system reduces the same partials in the same order: alpha =
-//   r'z / p'Ap, and for r_new = r - alpha Ap, without another reduction,
+//   Phase A, one warp per row (iy, iz) of control points, lanes along x: Ap = the node sum of the
+//   brick partials plus the sparse term, output rule applied; and five dot products p'Ap, z'Ap,
+//   Ap'D^-1 Ap, r'Ap, Ap'Ap (z = D^-1 r).  The loads of a node (its <= 8 brick partials per
+//   component, p, r, D^-1, the mask) are issued together.
+//   Barrier.  Every CTA of the system reduces the same partials in the same order: the phase A
+//   sums, and the exact r'r and r'z of the current r from the previous launch's phase B (or the
+//   state's after an initialisation or replacement).  alpha = r'z / p'Ap, and for
+//   r_new = r - alpha Ap, without another reduction,
 //       |r_new|^2 = r'r - 2 alpha r'Ap + alpha^2 Ap'Ap,
 //       r_new' D^-1 r_new = r'z - 2 alpha z'Ap + alpha^2 Ap'D^-1 Ap,
 //   which give the convergence test and beta = r_new'z_new / r'z.  When the FP32 residual has
 //   gained the replacement factor (or the segment is long) the state asks the host for an FP64
 //   residual replacement instead.
-//   Phase B: x += alpha p, r -= alpha Ap, p = D^-1 r + beta p (when the iteration goes on) with
-//   the next apply's input pin (p with the fixed DOFs zeroed, rows padded), and the exact r'r and
-//   r'z of the new r as per-CTA partials, which the next launch reduces in place of the formulas
-//   (so they bridge one iteration only).
+//   Phase B, four elements per thread at a time: x += alpha p, r -= alpha Ap, p = D^-1 r + beta p
+//   (when the iteration goes on) with the next apply's input pin (p with the fixed DOFs zeroed,
+//   rows padded), and the exact r'r and r'z of the new r as per-CTA partials.  Those partials
+//   alternate between two buffers by iteration parity, so a CTA that writes them never meets one
+//   that still reads the previous ones.
 // The system's first CTA writes its state.  All CTAs of a system take the same branches; the CTAs
 // of a stopped system only arrive at the barrier.
 __global__ void __launch_bounds__(kTailThreads, 4)
@@ -824,82 +830,102 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
     float *__restrict__ p = I.p;
     float *__restrict__ pin = I.pin;
     float *__restrict__ ap = I.ap;
-    double *pa = I.part, *pb = I.part + 5 * G;   // phase A partials [5][G], exact r'r, r'z [2][G]
-    // exact r'r and r'z of the current r: from the state after an initialisation or replacement,
-    // else from the previous launch's phase B
-    double rr0 = S.rr_old, rz0 = S.rz_old;
-    if (!S.fresh) {
-        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int i = threadIdx.x; i < G; i += blockDim.x) {
-            v[0] += __ldcg(pb + i);
-            v[1] += __ldcg(pb + G + i);
-        }
-        block_sum5(v);
-        rr0 = v[0];
-        rz0 = v[1];
-    }
-    const long long T = (long long)G * blockDim.x;
-    const long long t0 = (long long)bid * blockDim.x + threadIdx.x;
-    const long long n = 3 * g.nsc;
-    // A. Ap at every node and the five dot products; one warp per row (iy, iz) of control points,
-    // lanes along x, so the row's bricks are found once and neighbouring lanes read neighbouring
-    // partials
+    // partials: phase A [5][G]; exact r'r, r'z [2][G] in two buffers by iteration parity
+    const int par = int(S.iter & 1);
+    double *pa = I.part, *pb_new = I.part + (5 + 2 * par) * G, *pb_old = I.part + (7 - 2 * par) * G;
+    // 32-bit indices: the set-up keeps the padded vectors below 2^31 values
+    const int T = G * (int)blockDim.x;
+    const int t0 = bid * (int)blockDim.x + (int)threadIdx.x;
+    const int n = 3 * (int)g.nsc, nsc = (int)g.nsc;
+    // A. Ap at every node and the five dot products
     double dA[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const float *__restrict__ patch = I.patch;
     {
         const int lane = threadIdx.x & 31;
         const int nrows = g.cy * g.cz;
         const int wstride = (G * (int)blockDim.x) >> 5;
+        const size_t bstride = (size_t)3 * kPVol;
         for (int row = (bid * (int)blockDim.x + (int)threadIdx.x) >> 5; row < nrows; row += wstride) {
             const int iy = row % g.cy, iz = row / g.cy;
             int by[2], ly[2], bz[2], lz[2];
             const int nby = node_bricks(iy, kBY, g.nby, by, ly);
             const int nbz = node_bricks(iz, kBZ, g.nbz, bz, lz);
+            // the row's partial rows in the y bricks (absent ones repeat the first and are not added)
+            const size_t ybase0 = (size_t)g.nbx * by[0] * bstride + ly[0] * kPX;
+            const size_t ybase1 = (size_t)g.nbx * by[nby - 1] * bstride + ly[nby - 1] * kPX;
             for (int ix = lane; ix < g.cx; ix += 32) {
-                const long long nd = (long long)row * g.cx + ix;
-                int bx[2], lx[2];
-                const int nbx = node_bricks(ix, kBX, g.nbx, bx, lx);
+                const int nd = row * g.cx + ix;
+                const int bx1 = min(ix / kBX, g.nbx - 1), lx1 = ix - bx1 * kBX;
+                const bool two = lx1 <= 1 && bx1 >= 1;   // also in the previous brick along x
+                const int o1 = bx1 * (3 * kPVol) + lx1, o0 = two ? (bx1 - 1) * (3 * kPVol) + lx1 + kBX : o1;
                 float sv[3] = {0.f, 0.f, 0.f};
-                for (int a = 0; a < nbz; ++a)
-                    for (int q = 0; q < nby; ++q)
-                        for (int w = 0; w < nbx; ++w) {
-                            const size_t brick = (size_t)bx[w] + (size_t)g.nbx * (by[q] + (size_t)g.nby * bz[a]);
-                            const float *pq = patch + brick * 3 * kPVol + (lz[a] * kPY + ly[q]) * kPX + lx[w];
-                            sv[0] += pq[0];
-                            sv[1] += pq[kPVol];
-                            sv[2] += pq[2 * kPVol];
+                for (int a = 0; a < nbz; ++a) {   // z bricks, then y bricks, then x bricks: lower first
+                    const float *zb = patch + (size_t)g.nbx * g.nby * bz[a] * bstride + lz[a] * (kPY * kPX);
+                    float lo[2][3], hi[2][3];
+#pragma unroll
+                    for (int q2 = 0; q2 < 2; ++q2)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const float *rb = zb + (q2 ? ybase1 : ybase0) + c * kPVol;
+                            lo[q2][c] = rb[o0];
+                            hi[q2][c] = rb[o1];
                         }
 #pragma unroll
+                    for (int q2 = 0; q2 < 2; ++q2)
+                        if (q2 < nby)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                if (two) sv[c] += lo[q2][c];
+                                sv[c] += hi[q2][c];
+                            }
+                }
+                float pv[3], rr[3], iv[3];
+                bool mk[3];
+#pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const long long idx = (long long)c * g.nsc + nd;
+                    const int idx = c * nsc + nd;
+                    pv[c] = p[idx];
+                    rr[c] = r[idx];
+                    iv[c] = inv[idx];
+                    mk[c] = mask_mode == ICC_MASK_NONE || mask[idx];
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int idx = c * nsc + nd;
                     float v = sv[c];
                     if (I.sp.ptr) v += sparse_row(I.sp, idx, p, mask, mask_mode);
-                    if (mask_mode == ICC_MASK_ZERO && !mask[idx]) v = 0.f;
-                    else if (mask_mode == ICC_MASK_IDENTITY && !mask[idx]) v = p[idx];
+                    if (!mk[c]) v = mask_mode == ICC_MASK_ZERO ? 0.f : pv[c];
                     ap[idx] = v;
-                    const float ri = r[idx], iv = inv[idx];
                     const double av = double(v);
-                    dA[0] += double(p[idx]) * av;
-                    dA[1] += double(iv * ri) * av;
-                    dA[2] += double(iv * v) * av;
-                    dA[3] += double(ri) * av;
+                    dA[0] += double(pv[c]) * av;
+                    dA[1] += double(iv[c] * rr[c]) * av;
+                    dA[2] += double(iv[c] * v) * av;
+                    dA[3] += double(rr[c]) * av;
                     dA[4] += av * av;
                 }
             }
         }
     }
-    block_sum5(dA);
+    block_sum_n<5>(dA);
     if (threadIdx.x == 0)
 #pragma unroll
         for (int k = 0; k < 5; ++k) pa[k * G + bid] = dA[k];
     if (!grid_sync(ctr, err, wait_limit)) return;
     {
-        double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        for (int i = threadIdx.x; i < G; i += blockDim.x)
+        double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int i = threadIdx.x; i < G; i += blockDim.x) {
 #pragma unroll
             for (int k = 0; k < 5; ++k) v[k] += __ldcg(pa + k * G + i);
-        block_sum5(v);
+            if (!S.fresh) {
+                v[5] += __ldcg(pb_old + i);
+                v[6] += __ldcg(pb_old + G + i);
+            }
+        }
+        block_sum_n<7>(v);
         if (threadIdx.x == 0) {
+            // exact r'r and r'z of the current r: from the state after an initialisation or
+            // replacement, else from the previous launch's phase B
+            const double rr0 = S.fresh ? S.rr_old : v[5], rz0 = S.fresh ? S.rz_old : v[6];
             // rust/src/solver.rs:41-51 (alpha or breakdown), :56-71 (residual test, beta)
             S.iter += 1;
             S.p_ap = v[0];
@@ -934,39 +960,61 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
     }
     __syncthreads();
     if (s_stat == kStatBreakdown || s_stat == kStatNan) return;
-    // B. x += alpha p, r -= alpha Ap; the direction only when the iteration goes on
+    // B. x += alpha p, r -= alpha Ap; the direction only when the iteration goes on.  Element i of
+    // pin sits at i + (i / cx) (cxp - cx); the quotient and remainder are carried along.
     const float alpha = float(s_ab[0]), beta = float(s_ab[1]);
     const bool go = s_stat == 0;
     const bool ident = mask_mode == ICC_MASK_IDENTITY;
-    // index of i in the padded layout: i + (i / cx) (cxp - cx), the quotient kept up to date
-    const long long pad = I.cxp - g.cx, Tq = T / g.cx, Tr = T % g.cx;
-    long long row = t0 / g.cx, col = t0 % g.cx;
-    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (long long i = t0; i < n; i += T) {
-        const float pi = p[i];
-        x[i] += alpha * pi;
-        const float ri = r[i] - alpha * ap[i];
-        r[i] = ri;
-        const float zi = inv[i] * ri;
-        v[0] += double(ri) * double(ri);
-        v[1] += double(ri) * double(zi);
-        if (go) {
-            const float w = zi + beta * pi;
-            const float wm = (mask && !mask[i]) ? 0.f : w;
-            p[i] = ident ? w : wm;
-            pin[i + row * pad] = wm;
+    const int pad = I.cxp - g.cx, Tq = T / g.cx, Tr = T % g.cx;
+    int qrow = t0 / g.cx, qcol = t0 % g.cx;
+    constexpr int kU = 4;
+    double v[2] = {0.0, 0.0};
+    for (int i0 = t0; i0 < n; i0 += kU * T) {
+        float pv[kU], xv[kU], rv[kU], av[kU], iv[kU];
+        bool ok[kU], mk[kU];
+        int pidx[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            const int i = i0 + k * T;
+            ok[k] = i < n;
+            pidx[k] = i + qrow * pad;
+            qrow += Tq;
+            qcol += Tr;
+            if (qcol >= g.cx) {
+                qcol -= g.cx;
+                ++qrow;
+            }
+            if (ok[k]) {
+                pv[k] = p[i];
+                xv[k] = x[i];
+                rv[k] = r[i];
+                av[k] = ap[i];
+                iv[k] = inv[i];
+                mk[k] = !mask || mask[i];
+            }
         }
-        row += Tq;
-        col += Tr;
-        if (col >= g.cx) {
-            col -= g.cx;
-            ++row;
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+            if (!ok[k]) continue;
+            const int i = i0 + k * T;
+            x[i] = xv[k] + alpha * pv[k];
+            const float ri = rv[k] - alpha * av[k];
+            r[i] = ri;
+            const float zi = iv[k] * ri;
+            v[0] += double(ri) * double(ri);
+            v[1] += double(ri) * double(zi);
+            if (go) {
+                const float w = zi + beta * pv[k];
+                const float wm = mk[k] ? w : 0.f;
+                p[i] = ident ? w : wm;
+                pin[pidx[k]] = wm;
+            }
         }
     }
-    block_sum5(v);
+    block_sum_n<2>(v);
     if (threadIdx.x == 0) {
-        pb[bid] = v[0];
-        pb[G + bid] = v[1];
+        pb_new[bid] = v[0];
+        pb_new[G + bid] = v[1];
     }
 }
 
@@ -1215,7 +1263,7 @@ static int vecset_alloc(const Op &op, VecSet &v, int part_cap) {
     double **f64[] = {&v.x64, &v.r64, &v.y64};
     for (double **p : f64)
         if ((rc = dalloc(p, n, "alloc mixed"))) return rc;
-    if ((rc = dalloc(&v.part, (size_t)7 * part_cap, "alloc mixed"))) return rc;
+    if ((rc = dalloc(&v.part, (size_t)9 * part_cap, "alloc mixed"))) return rc;
     v.part_cap = part_cap;
     return ICC_OK;
 }
@@ -1249,7 +1297,8 @@ static void append_descs(const Op &op, int inst, std::vector<BrickDesc> &out) {
 
 static int mixed_init(Op &op) {
     if (op.mixed && op.mixed->ready) return ICC_OK;
-    if (op.g.nsc >= (1LL << 31)) return set_error(ICC_BAD_ARG, "tensor-core path: more than 2^31 control points");
+    if (3LL * ((op.g.cx + 3) & ~3) * op.g.cy * op.g.cz + 4LL * kTailThreads * 1024 >= (1LL << 31))
+        return set_error(ICC_BAD_ARG, "tensor-core path: more than 2^31 DOF");
     if (op.g.nbx > 2047 || op.g.nby > 2047 || op.g.nbz > 2047)
         return set_error(ICC_BAD_ARG, "tensor-core path: more than 2047 bricks along a direction");
     if (!op.mixed) op.mixed = new MixedState();
