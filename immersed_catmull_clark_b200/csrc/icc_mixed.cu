@@ -312,6 +312,38 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
              *fin = bars + 9, *p_full = bars + 10, *p_empty = bars + 10 + kNPatch, *t_full = bars + 10 + 2 * kNPatch;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, kPtTmemCols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        tc::mbar_init(&a_full[0], kRoleThreads);
+        tc::mbar_init(&a_full[1], kRoleThreads);
+        tc::mbar_init(&a_empty[0], 1);
+        tc::mbar_init(&a_empty[1], 1);
+        tc::mbar_init(&d_full[0], 1);
+        tc::mbar_init(&d_full[1], 1);
+        tc::mbar_init(&d_empty[0], kRoleThreads);
+        tc::mbar_init(&d_empty[1], kRoleThreads);
+        tc::mbar_init(b_full, 1);
+        tc::mbar_init(fin, 1);
+        for (int b = 0; b < kNPatch; ++b) {
+            tc::mbar_init(&p_full[b], 96);
+            tc::mbar_init(&p_empty[b], kRoleThreads);
+            tc::mbar_init(&t_full[b], 1);
+        }
+        tc::fence_mbar_init();
+        s_abort = 0;
+        // B, the same in every launch, is copied before the wait below
+        tc::mbar_arrive_expect_tx(b_full, kBBytes);
+        tc::bulk_g2s(sB, bmat, kBBytes, b_full);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    // everything below reads or writes what the previous kernel of the stream may still use (the
+    // states, the input, the brick partials)
+    tc::griddep_wait();
     {
         // stream compaction, kPtThreads candidates per round: each warp ballots its 32, the counts
         // give every warp its offset, the list keeps the order of the bricks
@@ -346,36 +378,18 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             }
             __syncthreads();
         }
-        if (s_nlist == 0) return;   // nothing for this CTA (the same for all its threads)
+        if (s_nlist == 0) {   // nothing for this CTA (the same for all its threads)
+            if (tid == 0) tc::mbar_wait_bounded(b_full, 0u, kWaitLimit);   // the B copy has landed
+            tc::fence_before_sync();
+            __syncthreads();
+            if (warp == 0) {
+                tc::fence_after_sync();
+                tc::tmem_dealloc(tmem_base, kPtTmemCols);
+            }
+            return;
+        }
     }
     const int nmine = s_nlist;
-
-    if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, kPtTmemCols);
-        tc::tmem_relinquish();
-    }
-    if (tid == 0) {
-        tc::mbar_init(&a_full[0], kRoleThreads);
-        tc::mbar_init(&a_full[1], kRoleThreads);
-        tc::mbar_init(&a_empty[0], 1);
-        tc::mbar_init(&a_empty[1], 1);
-        tc::mbar_init(&d_full[0], 1);
-        tc::mbar_init(&d_full[1], 1);
-        tc::mbar_init(&d_empty[0], kRoleThreads);
-        tc::mbar_init(&d_empty[1], kRoleThreads);
-        tc::mbar_init(b_full, 1);
-        tc::mbar_init(fin, 1);
-        for (int b = 0; b < kNPatch; ++b) {
-            tc::mbar_init(&p_full[b], 96);
-            tc::mbar_init(&p_empty[b], kRoleThreads);
-            tc::mbar_init(&t_full[b], 1);
-        }
-        tc::fence_mbar_init();
-        s_abort = 0;
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
 
     if (warp < kRoleWarps) {
@@ -621,8 +635,6 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     } else if (lane == 0) {
         // ------------------------------ MMA issuer ------------------------------
         constexpr uint32_t idesc = tc::idesc_tf32(kTcM, kTcN);
-        tc::mbar_arrive_expect_tx(b_full, kBBytes);
-        tc::bulk_g2s(sB, bmat, kBBytes, b_full);
         const bool b_ok = pt_wait(b_full, 0u, &s_abort, err);
         bool run = b_ok;
         // descriptors of K step 0 (hi and lo terms); the shared-memory window is below 256 KB,
@@ -959,6 +971,7 @@ pcg_tail_kernel(const TcInst *__restrict__ insts, int ninst, unsigned long long 
         }
     }
     __syncthreads();
+    tc::griddep_launch_dependents();   // the next apply may be scheduled (it waits for this grid)
     if (s_stat == kStatBreakdown || s_stat == kStatNan) return;
     // B. x += alpha p, r -= alpha Ap; the direction only when the iteration goes on.  Element i of
     // pin sits at i + (i / cx) (cxp - cx); the quotient and remainder are carried along.
@@ -1444,10 +1457,21 @@ static TcInst make_inst(const Op &op, const VecSet &v, PcgState *st, int cta0, i
     return I;
 }
 
-static void launch_apply_tc(cudaStream_t s, const TcInst *d_insts, int ninst, int nbricks, const BrickDesc *d_desc,
-                            const float4 *bmat, int *err, int num_sms) {
-    const int grid = std::min(num_sms, nbricks);
-    apply_tc_kernel<<<grid, kPtThreads, kPtSmem, s>>>(d_insts, ninst, nbricks, d_desc, bmat, err);
+// The apply may start while the previous kernel of the stream finishes (programmatic dependent
+// launch): it sets up TMEM, its barriers and the B copy, then waits for that kernel.
+static cudaError_t launch_apply_tc(cudaStream_t s, const TcInst *d_insts, int ninst, int nbricks,
+                                   const BrickDesc *d_desc, const float4 *bmat, int *err, int num_sms) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)std::min(num_sms, nbricks));
+    cfg.blockDim = dim3(kPtThreads);
+    cfg.dynamicSmemBytes = kPtSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, apply_tc_kernel, d_insts, ninst, nbricks, d_desc, bmat, err);
 }
 
 static cudaError_t launch_tail(cudaStream_t s, const TcInst *d_insts, int ninst, int grid, unsigned long long *ctr,
@@ -1472,7 +1496,8 @@ static int enqueue_apply_tc(Op &op, const float *x, float *y) {
     enqueue_pad_input(op, ms.v, x, op.stream);
     const TcInst I = make_inst(op, ms.v, nullptr, 0, 0, 1.f);
     ICC_CUDA(cudaMemcpyAsync(ms.d_inst, &I, sizeof(TcInst), cudaMemcpyHostToDevice, op.stream), "instance table");
-    launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms);
+    ICC_CUDA(launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms),
+             "tc apply launch");
     gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
                                                                        op.mask_mode, op.extra32(), y, nullptr, nullptr);
     ICC_CUDA(cudaGetLastError(), "tc apply launch");
@@ -1534,7 +1559,8 @@ int mixed_profile_apply(Op &op, const float *x, float *y, int reps, double *cont
     for (auto &e : ev) ICC_CUDA(cudaEventCreate(&e), "event create");
     for (int r = 0; r < reps; ++r) {
         cudaEventRecord(ev[3 * r], op.stream);
-        launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms);
+        ICC_CUDA(launch_apply_tc(op.stream, ms.d_inst, 1, op.g.nbricks, ms.d_desc, ms.d_bmat, ms.d_err, op.num_sms),
+                 "tc apply launch");
         cudaEventRecord(ev[3 * r + 1], op.stream);
         gather_kernel<float><<<op.vec_blocks, kVecThreads, 0, op.stream>>>(op.g, ms.v.patch32, x, op.d_mask,
                                                                            ICC_MASK_NONE, op.extra32(), y, nullptr,
@@ -1855,8 +1881,9 @@ static int capture_graph(MixedBatch &bt, int check_every) {
     ICC_CUDA(cudaStreamBeginCapture(bt.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t ce = cudaSuccess;
     for (int i = 0; i < check_every && ce == cudaSuccess; ++i) {
-        launch_apply_tc(bt.stream, bt.d_inst, bt.ninst, bt.nbricks, bt.d_desc, bt.bmat, bt.d_err, bt.num_sms);
-        ce = launch_tail(bt.stream, bt.d_inst, bt.ninst, bt.tail_grid, bt.d_ctr, bt.d_err, bt.limit);
+        ce = launch_apply_tc(bt.stream, bt.d_inst, bt.ninst, bt.nbricks, bt.d_desc, bt.bmat, bt.d_err, bt.num_sms);
+        if (ce == cudaSuccess)
+            ce = launch_tail(bt.stream, bt.d_inst, bt.ninst, bt.tail_grid, bt.d_ctr, bt.d_err, bt.limit);
     }
     cudaError_t ee = cudaStreamEndCapture(bt.stream, &graph);
     ICC_CUDA(ce, "capture fused vector step");

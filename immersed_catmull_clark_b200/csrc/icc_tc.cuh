@@ -186,6 +186,12 @@ __device__ __forceinline__ void tma_load_4d(void *dst_smem, const void *tmap, in
         : "memory");
 }
 
+// Programmatic dependent launch: wait until the grids this one depends on have completed and their
+// memory is visible (returns at once for a kernel launched without the attribute), and allow the
+// dependents of this grid to be scheduled.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // A tensor map written to global memory by the host: acquire it for the async proxy before use.
 __device__ __forceinline__ void fence_tensormap_acquire(const void *tmap) {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(tmap))
