@@ -303,15 +303,22 @@ def run_batched(args, wl):
     work = float(np.sum(ndofs * its))
     value = work / (np.mean(ms) * 1e-3)
 
-    def sequential():
+    def sequential(precision):
         out = []
         for op, b, n in zip(ops, bs, ndofs):
-            x, it, r = icc.PcgSolver(100000, TOL).solve(int(n), b, None, op)
+            x, it, r = icc.PcgSolver(100000, TOL, precision=precision).solve(int(n), b, None, op)
             out.append((x, it))
         return out
-    sequential()
-    ms64, seq = timed(sequential, 1)
+    sequential(icc.FP64)
+    ms64, seq = timed(lambda: sequential(icc.FP64), 1)
     err = max(float(np.linalg.norm(x - xr) / np.linalg.norm(xr)) for x, (xr, _) in zip(xs, seq))
+    # controls that separate the gain of batching from the gain of precision: the same 64 mixed
+    # solves one after another, and the 64 FP64 solves as one batched call
+    sequential(icc.MIXED)
+    ms_seq_mixed, _ = timed(lambda: sequential(icc.MIXED), 1)
+    batched64 = lambda: icc.solve_batched(ops, bs, tol=TOL, max_iter=100000, precision=icc.FP64)
+    batched64()
+    ms_bat64, (_, _, _, st64) = timed(batched64, 1)
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": float(np.mean(ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "tf32x3+f32+f64", "data": "synthetic",
@@ -321,7 +328,12 @@ def run_batched(args, wl):
                       "all_converged": bool(np.all(st == icc.ICC_OK)), "time_to_tol_ms": ms,
                       "vs_sequential_fp64": {"sequential_fp64_ms": ms64[0],
                                              "speedup": ms64[0] / float(np.mean(ms)),
-                                             "max_disp_rel_l2_vs_fp64_1e-8": err}},
+                                             "max_disp_rel_l2_vs_fp64_1e-8": err},
+                      "controls": {"sequential_mixed_ms": ms_seq_mixed[0],
+                                   "batching_gain_mixed": ms_seq_mixed[0] / float(np.mean(ms)),
+                                   "batched_fp64_ms": ms_bat64[0],
+                                   "batched_fp64_all_converged": bool(np.all(st64 == icc.ICC_OK)),
+                                   "precision_gain_batched": ms_bat64[0] / float(np.mean(ms))}},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(8 * ndofs.sum()),
                    "d2h_bytes_per_step": int(8 * ndofs.sum())},
            "clocks": clk.summary()}

@@ -395,7 +395,8 @@ class CantileverTopOpt:
             self._h = None
 
     def set_loads(self, forces):
-        """Load cases as simultaneous right-hand sides (rows of forces, each of ndof)."""
+        """Load cases (rows of forces, each of ndof).  In the mixed precision their state solves run as
+        one batch (one tensor-core apply over all cases per PCG iteration); in FP64 one after another."""
         f = np.ascontiguousarray(np.atleast_2d(forces), dtype=np.float64)
         _check(lib().icc_topopt_set_loads(self._h, f.shape[0], f.reshape(-1)))
 

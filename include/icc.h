@@ -197,10 +197,13 @@ typedef struct icc_topopt icc_topopt;
 int icc_topopt_create(const int64_t nel[3], const icc_topopt_cfg *cfg, icc_topopt **out);
 void icc_topopt_destroy(icc_topopt *t);
 
-/* Load cases as simultaneous right-hand sides (extends the reference's single tip load, which the
- * handle starts with): forces is nload x ndof (component-blocked, like every vector here).  Each
- * design iteration then solves every case warm-started from its previous state; compliance and
- * element energies are summed over the cases, and pcg_iters reports the sum. */
+/* Several load cases (extends the reference's single tip load, which the handle starts with):
+ * forces is nload x ndof (component-blocked, like every vector here).  Each design iteration then
+ * solves every case warm-started from its previous state.  With cfg.precision = ICC_MIXED and
+ * nload > 1 the cases' state solves run as one batch: every PCG iteration is one tensor-core
+ * apply over the bricks of all cases and one fused vector step (per-case PCG scalars, each case
+ * stops on its own tolerance).  With ICC_FP64 the cases are solved one after another.
+ * Compliance and element energies are summed over the cases, and pcg_iters reports the sum. */
 int icc_topopt_set_loads(icc_topopt *t, int32_t nload, const double *forces);
 
 /* rust/src/topopt_iga.rs:187-234 CantileverTopOpt::run: densities from volfrac, per iteration the
