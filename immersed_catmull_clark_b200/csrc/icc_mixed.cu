@@ -155,7 +155,7 @@ struct MixedState {
 //     shared buffer (z), transform the node partials of bricks at the grid's ends by E, and
 //     write the brick partials.
 // mbarriers: t_full (TMA copies), p_full/p_empty (patch buffers), a_full/a_empty (A slots),
-// d_full/d_empty (two accumulator buffers), b_full, fin.
+// d_full/d_empty (kNAcc accumulator buffers), b_full, fin.
 // Every wait is bounded.  On time-out the waiting thread raises a shared abort flag; every other
 // wait then returns false at once.  The builders and the epilogue decide at a barrier that ORs
 // the flag over the role, so all threads of a role leave their loop at the same brick; the MMA
@@ -167,9 +167,11 @@ constexpr int kMmaWarp = 2 * kRoleWarps, kLoaderWarp = 2 * kRoleWarps + 1;
 constexpr int kPtThreads = (2 * kRoleWarps + 4) * 32;
 constexpr int kColSlot = kTcK;         // A_hi slot s: TMEM columns s*96 + [0,96)
 constexpr int kColD = 2 * kColSlot;    // accumulator buffer d: TMEM columns 192 + d*96 + [0,96)
+constexpr int kNAcc = 3;              // accumulator buffers: the epilogue may lag the MMA by two bricks
 constexpr int kAloFl = kTcM * kTcK;    // A_lo slot (shared memory, canonical K-major): floats
 constexpr uint32_t kALbo = (kTcM / 8) * 128;  // bytes between K-adjacent core matrices of A_lo
 constexpr uint32_t kPtTmemCols = 512;
+static_assert(kColD + kNAcc * kTcN <= (int)kPtTmemCols, "accumulators beyond the TMEM allocation");
 constexpr int kZFl = kBZ * 3 * 3 * kPY * kPX;  // per-layer node partials: [lz][az][c][py][px]
 constexpr int kPXs = 12;                        // x extent of an input patch row in shared memory (48 B)
 constexpr int kPVolS = kPZ * kPY * kPXs;        // per component
@@ -301,7 +303,7 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     float *sP = sAlo + 2 * kAloFl;        // [kNPatch][kPatBuf] input patches
     float *sZb = sP + kNPatch * kPatBuf;  // [2][kZFl] per-layer node partials, by brick parity
     float *sW = sZb + 2 * kZFl;           // [3 * kPVol] node partials of a boundary brick (E applied)
-    __shared__ __align__(8) uint64_t bars[10 + 3 * kNPatch];
+    __shared__ __align__(8) uint64_t bars[6 + 2 * kNAcc + 3 * kNPatch];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int s_abort;
     // this CTA's bricks of systems whose solve goes on: bricks blockIdx.x + k gridDim.x in order
@@ -309,8 +311,10 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
     __shared__ int s_cnt[32];
     __shared__ int s_nlist;
     __shared__ unsigned s_act[kMaxInst / 32];   // bit i: system i's solve goes on
-    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 6, *b_full = bars + 8,
-             *fin = bars + 9, *p_full = bars + 10, *p_empty = bars + 10 + kNPatch, *t_full = bars + 10 + 2 * kNPatch;
+    uint64_t *a_full = bars, *a_empty = bars + 2, *d_full = bars + 4, *d_empty = bars + 4 + kNAcc,
+             *b_full = bars + 4 + 2 * kNAcc,
+             *fin = bars + 5 + 2 * kNAcc, *p_full = bars + 6 + 2 * kNAcc, *p_empty = p_full + kNPatch,
+             *t_full = p_full + 2 * kNPatch;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
         tc::tmem_alloc(&tmem_base, kPtTmemCols);
@@ -321,10 +325,10 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         tc::mbar_init(&a_full[1], kRoleThreads);
         tc::mbar_init(&a_empty[0], 1);
         tc::mbar_init(&a_empty[1], 1);
-        tc::mbar_init(&d_full[0], 1);
-        tc::mbar_init(&d_full[1], 1);
-        tc::mbar_init(&d_empty[0], kRoleThreads);
-        tc::mbar_init(&d_empty[1], kRoleThreads);
+        for (int d = 0; d < kNAcc; ++d) {
+            tc::mbar_init(&d_full[d], 1);
+            tc::mbar_init(&d_empty[d], kRoleThreads);
+        }
         tc::mbar_init(b_full, 1);
         tc::mbar_init(fin, 1);
         for (int b = 0; b < kNPatch; ++b) {
@@ -472,19 +476,22 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             zb[k] = 9 * (kPY * kPX) * pz + (kPY * kPX) * ci + pyx;
             zpz[k] = pz;
         }
-        for (int it = 0; it < nmine; ++it) {
+        for (int it = 0, db = 0, dph = 0; it < nmine; ++it) {
             float *sZ = sZb + (it & 1) * kZFl;
-            const int db = it & 1;
             const BrickDesc d = desc[s_list[it]];
             // on a failed wait the values read below are not used: the barrier before the z-sum
             // makes every epilogue thread leave the loop
-            const bool ok = pt_wait(&d_full[db], uint32_t(it >> 1) & 1u, &s_abort, err);
+            const bool ok = pt_wait(&d_full[db], uint32_t(dph), &s_abort, err);
             tc::fence_after_sync();
             uint32_t dv[32];
             tc::tmem_ld32(dcol0 + (uint32_t)(db * kTcN), dv);
             tc::tmem_wait_ld();
             tc::fence_before_sync();
-            tc::mbar_arrive(&d_empty[db]);   // accumulator buffer db is free for brick it + 2
+            tc::mbar_arrive(&d_empty[db]);   // accumulator buffer db is free for brick it + kNAcc
+            if (++db == kNAcc) {
+                db = 0;
+                dph ^= 1;
+            }
             float res[27];
 #pragma unroll
             for (int a = 0; a < 27; ++a) res[a] = __uint_as_float(dv[a]);
@@ -641,12 +648,13 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
         // so adding a step's offset never carries out of the address field
         const uint64_t dbh0 = tc::make_desc(sB, kBLbo, kSbo), dbl0 = tc::make_desc(sB + kBFl, kBLbo, kSbo);
         const uint64_t dal0 = tc::make_desc(sAlo, kALbo, kSbo), dal1 = tc::make_desc(sAlo + kAloFl, kALbo, kSbo);
-        for (int it = 0; it < nmine && run; ++it) {
-            const int s = it & 1, db = it & 1;
-            // slot s holds brick it, and brick it - 2 has been drained from accumulator buffer db;
-            // on a failed wait nothing more is issued
+        for (int it = 0, db = 0, dph = 0; it < nmine && run; ++it) {
+            const int s = it & 1;
+            // slot s holds brick it, and brick it - kNAcc has been drained from accumulator buffer
+            // db (brick it is its use number it / kNAcc, dph the parity of that); on a failed wait
+            // nothing more is issued
             run = pt_wait(&a_full[s], uint32_t(it >> 1) & 1u, &s_abort, err) &&
-                  (it < 2 || pt_wait(&d_empty[db], uint32_t((it >> 1) - 1) & 1u, &s_abort, err));
+                  (it < kNAcc || pt_wait(&d_empty[db], uint32_t(dph ^ 1), &s_abort, err));
             if (!run) break;
             tc::fence_after_sync();
             const uint32_t acol = tmem + (uint32_t)(s * kColSlot);
@@ -664,10 +672,14 @@ apply_tc_kernel(const TcInst *__restrict__ insts, int ninst, int nbricks, const 
             }
             tc::mma_commit(&d_full[db]);
             tc::mma_commit(&a_empty[s]);
+            if (++db == kNAcc) {
+                db = 0;
+                dph ^= 1;
+            }
         }
         if (run)
-            for (int it = nmine - 2; it < nmine; ++it)
-                if (it >= 0 && !pt_wait(&d_empty[it & 1], uint32_t(it >> 1) & 1u, &s_abort, err)) break;
+            for (int it = nmine - kNAcc; it < nmine; ++it)
+                if (it >= 0 && !pt_wait(&d_empty[it % kNAcc], uint32_t(it / kNAcc) & 1u, &s_abort, err)) break;
         // every MMA this thread issued has completed once fin arrives; then TMEM may be released.
         // A B copy whose wait failed is waited for again, so it does not land after the CTA ends.
         tc::mma_commit(fin);
