@@ -183,14 +183,14 @@ static_assert(kPatBuf * 4 >= (int)kPatchBytes && (kPatBuf * 4) % 128 == 0, "patc
 constexpr int kPtSmem = (2 * kBFl + 2 * kAloFl + kNPatch * kPatBuf + 2 * kZFl + 3 * kPVol) * 4;  // 219,872 B
 constexpr uint32_t kBBytes = 2 * kBFl * 4;                         // hi + lo
 
-// Each test may sleep up to kWaitSleepNs; with kWaitLimit tests a wait gives up after at most
-// ~4 s, and after at least kWaitLimit quick tests (~0.1 s) if the hardware ignores the hint --
-// both far beyond any wait of a working kernel (a brick takes a few microseconds).
-constexpr uint32_t kWaitSleepNs = 1000;
-
+// A test (mbarrier.try_wait without a time hint) may suspend the thread for a system-dependent
+// time; after kWaitLimit tests (~0.1 s if they return at once, a few seconds if each suspends for
+// about a microsecond) the wait gives up -- far beyond any wait of a working kernel (a brick takes
+// a few microseconds).  Measured on the 128x64x64 apply, the version with a 1 us suspend hint
+// took 1% longer.
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err) {
     for (long long i = 0; i < kWaitLimit; ++i) {
-        if (tc::mbar_try_wait_sleep(bar, parity, kWaitSleepNs)) return true;
+        if (tc::mbar_try_wait(bar, parity)) return true;
         if (*abort_flag) return false;
     }
     *abort_flag = 1;

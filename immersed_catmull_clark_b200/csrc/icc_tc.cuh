@@ -67,21 +67,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// The same test, letting the thread sleep in the instruction until the phase completes or about
-// `ns` nanoseconds have passed (a hint: the hardware may return earlier), so a waiting warp does
-// not take issue slots from the working ones.
-__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity), "r"(ns)
-        : "memory");
-    return ok != 0;
-}
-
 // Bounded wait on an mbarrier phase; false when the iteration limit ran out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit) {
     for (long long i = 0; i < limit; ++i)
