@@ -163,7 +163,7 @@ struct MixedState {
 // of the CTA is in flight when TMEM is released.  The host reports ICC_TIMEOUT.
 constexpr int kRoleWarps = 12;                  // builders: warps 0-11, epilogue: 12-23, MMA: 24, loaders: 25-27
 constexpr int kRoleThreads = kRoleWarps * 32;
-constexpr int kMmaWarp = 2 * kRoleWarps, kLoaderWarp = 2 * kRoleWarps + 1;
+constexpr int kLoaderWarp = 2 * kRoleWarps + 1;   // the MMA warp is 2 kRoleWarps
 constexpr int kPtThreads = (2 * kRoleWarps + 4) * 32;
 constexpr int kColSlot = kTcK;         // A_hi slot s: TMEM columns s*96 + [0,96)
 constexpr int kColD = 2 * kColSlot;    // accumulator buffer d: TMEM columns 192 + d*96 + [0,96)

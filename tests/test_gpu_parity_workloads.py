@@ -1,23 +1,24 @@
-"""Parity at the benchmark configurations' own sizes and accuracy bars.
+"""Parity at the benchmark workloads' own sizes and accuracy bars.
 
 Every reference solution here is checked by the oracle (the CPU restatement of the reference's
 path), never by the device operator alone:
 
-* C1 (24x16x12 cantilever, 19,656 DOF): the oracle's CSR Jacobi-PCG (rust/src/solver.rs:14-76 on
+* cantilever24 (24x16x12 cantilever, 19,656 DOF): the oracle's CSR Jacobi-PCG (rust/src/solver.rs:14-76 on
   the AssemblyPattern matrix) solved to a recurrence residual of 1e-14 is the tight solution.  The
   device FP64 PCG at 1e-8 must be as close to it as the oracle's own PCG at 1e-8; the mixed solve
-  at 1e-8 must be within the north star's 1e-7 (displacement, relative L2) and its compliance too.
-* C2 (128x64x64, 1.70 M DOF) and C3 (96^3 cylinders, 2.82 M DOF): the oracle's CSR does not fit,
+  at 1e-8 must be within the 1e-7 accuracy target of the mixed form (displacement, relative L2)
+  and its compliance too.
+* cantilever128 (128x64x64, 1.70 M DOF) and cylinders96 (96^3 cylinders, 2.82 M DOF): the oracle's CSR does not fit,
   so the tight solution is the device FP64 PCG at 1e-12, accepted only when the oracle's
   matrix-free element loop confirms its true residual; the mixed solve must be within 1e-7 of it.
-* C4 (64 uneven designs): every instance of the batched mixed call against its own tight FP64
+* batched64 (64 uneven designs): every instance of the batched mixed call against its own tight FP64
   solution; the smallest designs also against the oracle's CSR solve.
-* C5 (multi-load SIMP loop): the device loop with four load cases against the oracle's loop on a
+* topopt (multi-load SIMP loop): the device loop with four load cases against the oracle's loop on a
   grid it runs quickly, and mixed against FP64 state solves at the configured 256x128x128.
 
 The accuracy bar of the mixed form (displacement and compliance within 1e-7 of the FP64 solution)
-is the north star's; the FP64 bars are derived from the reference algorithm's own accuracy at the
-same tolerance.
+is its accuracy target; the FP64 bars are derived from the reference algorithm's own accuracy at
+the same tolerance.
 """
 import numpy as np
 import pytest
@@ -29,7 +30,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-8
-MIXED_DISP = 1e-7       # north star: displacement error of the mixed form vs the FP64 solution
+MIXED_DISP = 1e-7       # target: displacement error of the mixed form vs the FP64 solution
 MIXED_COMP = 1e-7       # and its compliance error
 
 
@@ -54,11 +55,11 @@ def oracle_true_residual(p, em, x, b):
 
 
 # ---------------------------------------------------------------------------------------------
-# C1: against the oracle's CSR solve
+# cantilever24: against the oracle's CSR solve
 
 
 @pytest.fixture(scope="module")
-def c1():
+def cant24():
     p = W.cantilever((24, 16, 12), seed=2026)
     osp = O.Space(p.bounds, p.nel, 2)
     sp, em, op = device_setup(p)
@@ -70,12 +71,12 @@ def c1():
     return dict(p=p, sp=sp, em=em, op=op, k=k, b=b, diag=diag, xt=xt, xo=xo, ito=ito)
 
 
-def test_c1_fp64_pcg_as_accurate_as_reference(c1):
-    sp, op, b, diag, xt, xo = c1["sp"], c1["op"], c1["b"], c1["diag"], c1["xt"], c1["xo"]
+def test_cantilever24_fp64_pcg_as_accurate_as_reference(cant24):
+    sp, op, b, diag, xt, xo = cant24["sp"], cant24["op"], cant24["b"], cant24["diag"], cant24["xt"], cant24["xo"]
     solver = icc.PcgSolver(20 * sp.ndof, TOL)
     x, it, res = solver.solve(sp.ndof, b, diag, op)
     assert solver.status == icc.ICC_OK and res < TOL
-    assert abs(it - c1["ito"]) <= max(3, 0.02 * c1["ito"]), (it, c1["ito"])
+    assert abs(it - cant24["ito"]) <= max(3, 0.02 * cant24["ito"]), (it, cant24["ito"])
     e_ref = rel(xo, xt)            # the reference algorithm's own error at this tolerance
     e_dev = rel(x, xt)
     assert e_dev <= 2.0 * e_ref + 1e-13, (e_dev, e_ref)
@@ -86,12 +87,12 @@ def test_c1_fp64_pcg_as_accurate_as_reference(c1):
     assert rel(xd, xt) < 1e-12
 
 
-def test_c1_mixed_within_north_star_bars(c1):
-    p, sp, op, b, diag, xt = c1["p"], c1["sp"], c1["op"], c1["b"], c1["diag"], c1["xt"]
+def test_cantilever24_mixed_within_accuracy_target(cant24):
+    p, sp, op, b, diag, xt = cant24["p"], cant24["sp"], cant24["op"], cant24["b"], cant24["diag"], cant24["xt"]
     solver = icc.PcgSolver(20 * sp.ndof, TOL, precision=icc.MIXED)
     xm, itm, resm = solver.solve(sp.ndof, b, diag, op)
     assert solver.status == icc.ICC_OK and resm < TOL
-    r_true = b - p.free_mask * c1["k"].matvec(p.free_mask * xm)
+    r_true = b - p.free_mask * cant24["k"].matvec(p.free_mask * xm)
     assert np.linalg.norm(r_true) / np.linalg.norm(b) < 1.5 * TOL
     assert rel(xm, xt) <= MIXED_DISP
     c_ref, c = p.force @ xt, p.force @ xm
@@ -99,7 +100,7 @@ def test_c1_mixed_within_north_star_bars(c1):
 
 
 # ---------------------------------------------------------------------------------------------
-# C2 and C3: tight device FP64 solutions confirmed by the oracle's element loop
+# cantilever128 and cylinders96: tight device FP64 solutions confirmed by the oracle's element loop
 
 
 def tight_fp64(p, em, op, b, diag):
@@ -125,7 +126,7 @@ def check_mixed_against(p, em, op, b, diag, xt):
     return d
 
 
-def test_c2_mixed_vs_tight_fp64_128x64x64():
+def test_cantilever128_mixed_vs_tight_fp64_128x64x64():
     p = W.cantilever((128, 64, 64), smooth=True, seed=2026)
     sp, em, op = device_setup(p)
     b = W.rhs_masked(p)
@@ -137,14 +138,14 @@ def test_c2_mixed_vs_tight_fp64_128x64x64():
 
 
 @pytest.fixture(scope="module")
-def c3():
+def cyl96():
     p = W.cylinders(96)
     sp, em, op = device_setup(p)
     return p, sp, em, op
 
 
-def test_c3_apply_probes_96(c3):
-    p, sp, em, op = c3
+def test_cylinders96_apply_probes_96(cyl96):
+    p, sp, em, op = cyl96
     osp = O.Space(p.bounds, p.nel, 2)
     rng = np.random.default_rng(96)
     x = rng.standard_normal(sp.ndof)
@@ -156,8 +157,8 @@ def test_c3_apply_probes_96(c3):
     assert rel(op.matvec_f32(x32), yo32) < 5e-6
 
 
-def test_c3_mixed_vs_tight_fp64_96(c3):
-    p, sp, em, op = c3
+def test_cylinders96_mixed_vs_tight_fp64_96(cyl96):
+    p, sp, em, op = cyl96
     b = W.rhs_masked(p)
     diag = np.maximum(op.diagonal(), 1e-6)    # the immersed clamp (rust/src/immersed.rs:555)
     xt = tight_fp64(p, em, op, b, diag)
@@ -165,10 +166,10 @@ def test_c3_mixed_vs_tight_fp64_96(c3):
 
 
 # ---------------------------------------------------------------------------------------------
-# C4: the configured 64 designs
+# batched64: the configured 64 designs
 
 
-def test_c4_batched_mixed_every_instance():
+def test_batched64_batched_mixed_every_instance():
     ks, probs = W.batched_designs(64, 8, 48, 2026)
     setups = [device_setup(p) for p in probs]
     ops = [s[2] for s in setups]
@@ -194,11 +195,11 @@ def test_c4_batched_mixed_every_instance():
 
 
 # ---------------------------------------------------------------------------------------------
-# C5: the multi-load SIMP loop
+# topopt: the multi-load SIMP loop
 
 
 @pytest.mark.parametrize("precision", [icc.FP64, icc.MIXED])
-def test_c5_multiload_loop_matches_oracle(precision):
+def test_topopt_multiload_loop_matches_oracle(precision):
     nel = [16, 8, 8]
     size = (2.0, 1.0, 1.0)
     loads = W.tip_load_cases(nel, size=size)
@@ -213,7 +214,7 @@ def test_c5_multiload_loop_matches_oracle(precision):
     assert np.abs(h.density - dens_o).max() < (1e-6 if precision == icc.FP64 else 1e-5)
 
 
-def test_c5_configured_size_mixed_vs_fp64():
+def test_topopt_configured_size_mixed_vs_fp64():
     nel = (256, 128, 128)
     size = (2.0, 1.0, 1.0)
     loads = W.tip_load_cases(nel, size=size)
