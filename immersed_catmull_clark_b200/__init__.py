@@ -39,7 +39,7 @@ FP64, MIXED = 0, 1
 # every symbol include/icc.h declares
 EXPORTED = [
     "icc_last_error", "icc_space_create", "icc_space_destroy", "icc_space_dims", "icc_space_connectivity",
-    "icc_lame", "icc_element_matrices", "icc_op_create", "icc_op_create_lame", "icc_op_destroy",
+    "icc_lame", "icc_element_matrices", "icc_space_window", "icc_op_create", "icc_op_create_lame", "icc_op_destroy",
     "icc_op_update_scale", "icc_op_update_mask", "icc_op_apply", "icc_op_apply_dev", "icc_op_apply_f32",
     "icc_op_apply_f32_dev", "icc_op_diagonal",
     "icc_op_stream", "icc_pcg_solve", "icc_pcg_solve_dev", "icc_op_last_solve_info", "icc_op_profile_apply",
@@ -93,6 +93,7 @@ def lib():
     L.icc_last_error.restype = C.c_char_p
     L.icc_space_create.argtypes = [f64p, i64p, i32, C.POINTER(vp)]
     L.icc_space_destroy.argtypes = [vp]
+    L.icc_space_window.argtypes = [vp, i64p, i64p, C.POINTER(vp)]
     L.icc_space_dims.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), i64p, i64p]
     L.icc_space_connectivity.argtypes = [vp, i64p]
     L.icc_lame.argtypes = [dbl, dbl, C.POINTER(dbl), C.POINTER(dbl)]
@@ -156,11 +157,14 @@ def lame(young, poisson):
 class SpaceBox:
     """p = 2 tensor-product B-spline space on a 3-D box (rust/src/iga/space.rs:107)."""
 
-    def __init__(self, bounds, nsub, degree=2):
-        b = np.ascontiguousarray(np.asarray(bounds, dtype=np.float64).reshape(-1))
-        ns = np.ascontiguousarray(np.asarray(nsub, dtype=np.int64))
-        h = C.c_void_p()
-        _check(lib().icc_space_create(b, ns, int(degree), C.byref(h)))
+    def __init__(self, bounds, nsub, degree=2, _handle=None):
+        if _handle is None:
+            b = np.ascontiguousarray(np.asarray(bounds, dtype=np.float64).reshape(-1))
+            ns = np.ascontiguousarray(np.asarray(nsub, dtype=np.int64))
+            h = C.c_void_p()
+            _check(lib().icc_space_create(b, ns, int(degree), C.byref(h)))
+        else:
+            h = _handle
         self._h = h
         ndof, nel = C.c_int64(), C.c_int64()
         nd = np.zeros(3, dtype=np.int64); ne = np.zeros(3, dtype=np.int64)
@@ -177,6 +181,18 @@ class SpaceBox:
         if h is not None and _lib is not None:
             _lib.icc_space_destroy(h)
             self._h = None
+
+    def window(self, e0, e1):
+        """The sub-grid of elements [e0[d], e1[d]) with this space's B-splines, numbered locally
+        (icc_space_window): the local space of a slab in the multi-rank solve."""
+        a = np.ascontiguousarray(np.asarray(e0, dtype=np.int64))
+        b = np.ascontiguousarray(np.asarray(e1, dtype=np.int64))
+        h = C.c_void_p()
+        _check(lib().icc_space_window(self._h, a, b, C.byref(h)))
+        nel = self.nel_dir
+        h_el = [(self.bounds[d, 1] - self.bounds[d, 0]) / nel[d] for d in range(3)]
+        bounds = np.array([[self.bounds[d, 0] + a[d] * h_el[d], self.bounds[d, 0] + b[d] * h_el[d]] for d in range(3)])
+        return SpaceBox(bounds, b - a, 2, _handle=h)
 
     def connectivity(self):
         c = np.zeros(self.nel * 81, dtype=np.int64)

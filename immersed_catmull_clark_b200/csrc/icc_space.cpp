@@ -270,6 +270,36 @@ int icc_space_create(const double bounds[6], const int64_t nsub[3], int32_t degr
     return ICC_OK;
 }
 
+// A sub-grid of a space: its elements [e0[d], e1[d]) per direction with the parent's B-splines
+// (the parent's knots, so the window's element matrices are the parent's, also next to a cut),
+// numbered locally: control points [e0, e1 + 2) of the parent, x fastest.
+int icc_space_window(const icc_space *sp, const int64_t e0[3], const int64_t e1[3], icc_space **out) {
+    if (!sp || !e0 || !e1 || !out) return set_error(ICC_BAD_ARG, "icc_space_window: null argument");
+    *out = nullptr;
+    const icc::Space &p = sp->s;
+    for (int d = 0; d < 3; ++d)
+        if (e0[d] < 0 || e1[d] <= e0[d] || e1[d] > p.nel_dir[d])
+            return set_error(ICC_BAD_ARG, "icc_space_window: element range outside the space");
+    auto *w = new (std::nothrow) icc_space();
+    if (!w) return set_error(ICC_OUT_OF_MEMORY, "icc_space_window: out of host memory");
+    icc::Space &s = w->s;
+    for (int d = 0; d < 3; ++d) {
+        const double h = p.len[d] / double(p.nel_dir[d]);
+        s.lo[d] = p.lo[d] + double(e0[d]) * h;
+        s.len[d] = double(e1[d] - e0[d]) * h;
+        s.nel_dir[d] = e1[d] - e0[d];
+        s.ncp[d] = s.nel_dir[d] + 2;
+        s.mats1d[d] = p.mats1d[d];
+        s.basis1d[d] = p.basis1d[d];
+        s.type1d[d].assign(p.type1d[d].begin() + e0[d], p.type1d[d].begin() + e1[d]);
+    }
+    s.nel = s.nel_dir[0] * s.nel_dir[1] * s.nel_dir[2];
+    s.nsc = s.ncp[0] * s.ncp[1] * s.ncp[2];
+    s.ndof = 3 * s.nsc;
+    *out = w;
+    return ICC_OK;
+}
+
 void icc_space_destroy(icc_space *sp) { delete sp; }
 
 int icc_space_dims(const icc_space *sp, int64_t *ndof, int64_t *nel, int64_t ndof_dir[3], int64_t nel_dir[3]) {

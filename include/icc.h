@@ -78,6 +78,12 @@ const char *icc_last_error(void);
  * box 3-D (the hot path); open uniform knots of maximal regularity (rust/src/iga/quadrature.rs:51). */
 int icc_space_create(const double bounds[6], const int64_t nsub[3], int32_t degree, icc_space **out);
 void icc_space_destroy(icc_space *sp);
+/* A sub-grid of a space (no reference counterpart; the domain decomposition of the multi-rank
+ * solve): elements [e0[d], e1[d]) per direction, 0 <= e0 < e1 <= nel_dir, with the parent's
+ * B-splines, numbered locally (control points [e0, e1 + 2) of the parent, x fastest).  Its element
+ * matrices (icc_element_matrices) are the parent's elements' matrices, including next to the cut,
+ * and operators on it run on the tensor cores as well. */
+int icc_space_window(const icc_space *sp, const int64_t e0[3], const int64_t e1[3], icc_space **out);
 /* ndof, nel, control points per direction, elements per direction */
 int icc_space_dims(const icc_space *sp, int64_t *ndof, int64_t *nel, int64_t ndof_dir[3], int64_t nel_dir[3]);
 /* SpaceBox::connectivity (rust/src/iga/space.rs:148-155): conn[e*81 + c*27 + a] */

@@ -75,3 +75,25 @@ def test_operator_fails_loudly_without_device():
     with pytest.raises(icc.IccError) as ei:
         icc.MatrixFreeOperator(sp, (lam, mu))
     assert ei.value.code in (icc.ICC_NO_DEVICE, icc.ICC_CUDA_ERROR)
+
+
+@pytest.mark.parametrize("e0,e1", [((0, 0, 0), (3, 4, 2)), ((2, 1, 0), (7, 4, 3)), ((4, 0, 1), (9, 4, 3))])
+def test_space_window_keeps_parent_matrices(e0, e1):
+    # a window of the space (the local space of a slab) has the parent's element matrices, also next
+    # to a cut inside the grid, and its local numbering covers the parent's control points [e0, e1 + 2)
+    sp = icc.SpaceBox(np.array([[0.0, 1.8], [0.0, 0.8], [0.0, 0.6]]), (9, 4, 3), 2)
+    lam, mu = icc.lame(1.0, 0.3)
+    em = icc.elasticity_element_matrices(sp, lam, mu)
+    w = sp.window(e0, e1)
+    assert w.nel_dir == [b - a for a, b in zip(e0, e1)]
+    assert w.ndof_dir == [b - a + 2 for a, b in zip(e0, e1)]
+    ew = icc.elasticity_element_matrices(w, lam, mu)
+    nx, ny, _ = sp.nel_dir
+    for ez in range(e0[2], e1[2]):
+        for ey in range(e0[1], e1[1]):
+            for ex in range(e0[0], e1[0]):
+                g = ex + nx * (ey + ny * ez)
+                l = (ex - e0[0]) + w.nel_dir[0] * ((ey - e0[1]) + w.nel_dir[1] * (ez - e0[2]))
+                assert np.array_equal(ew.types[ew.type_id[l]], em.types[em.type_id[g]])
+    with pytest.raises(icc.IccError):
+        sp.window((0, 0, 0), (10, 4, 3))

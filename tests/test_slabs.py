@@ -1,7 +1,8 @@
-"""The x-slab form of the FP64 PCG on two ranks (gloo, CPU): partitioning, the halo sum of the two
-shared control-point planes and the distributed reductions, with the oracle's element loop as each
-rank's local operator, against the single-domain oracle (rust/src/solver.rs:14-76 on the whole
-grid)."""
+"""The x-slab forms of the PCG on two and three ranks (gloo, CPU): partitioning, the halo sum of the
+two shared control-point planes and the distributed reductions, with the oracle's element loop as
+each rank's local operator, against the single-domain oracle (rust/src/solver.rs:14-76 on the whole
+grid).  The mixed-precision form runs its FP32 recurrence on the oracle's apply rounded to FP32
+(input and output), with FP64 residual replacement across the slabs."""
 import os
 import socket
 
@@ -81,6 +82,68 @@ def test_slab_pcg_matches_single_domain(world, nel):
         assert status == "ok" and res < 1e-10
         assert abs(it - ito) <= 2, (it, ito)
         assert sol_err < 1e-8, (rank, sol_err)
+
+
+def _rank_main_mixed(rank, world, port, nel, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    os.environ["OMP_NUM_THREADS"] = "1"
+    torch.set_num_threads(1)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from oracle import oracle as O
+        p = W.cantilever(nel, seed=11)
+        gsp = O.Space(p.bounds, p.nel, 2)
+        lam, mu = O.lame(1.0, 0.3)
+        types, tid, _ = gsp.element_matrices(lam, mu)
+        slab = S.Slab(rank, world, tuple(nel), *S.partition(nel[0], world)[rank])
+        lsp = O.Space(slab.bounds(p.bounds), (slab.e1 - slab.e0, nel[1], nel[2]), 2)
+        eids, dids = slab.element_ids(), slab.dof_ids()
+        ltid, lscale, lmask = tid[eids], p.scale[eids], p.free_mask[dids]
+
+        def apply64(x):
+            return torch.from_numpy(O.mf_apply(lsp, types, ltid, lscale, x.numpy(), lmask, 1))
+
+        def apply32(x):
+            y = O.mf_apply(lsp, types, ltid, lscale, x.numpy().astype(np.float64), lmask, 1)
+            return torch.from_numpy(y.astype(np.float32))
+
+        pcg = S.SlabMixedPcg(slab, apply64, apply32, torch.device("cpu"))
+        b = W.rhs_masked(p)
+        dg = np.maximum(O.mf_diagonal(gsp, types, tid, p.scale), 1e-12)
+        dl = torch.from_numpy(O.mf_diagonal(lsp, types, ltid, lscale))
+        pcg.halo.sum(dl)
+        dl = torch.clamp(dl, min=1e-12)
+        x, it, res, status = pcg.solve(torch.from_numpy(b[dids].copy()), dl, 20 * gsp.ndof, 1e-10)
+        # the single-domain FP64 solution, tight
+        xo, ito, _ = O.pcg_mf(gsp, types, tid, p.scale, b, dg, 40 * gsp.ndof, 1e-13, p.free_mask, 1)
+        _, ito10, _ = O.pcg_mf(gsp, types, tid, p.scale, b, dg, 20 * gsp.ndof, 1e-10, p.free_mask, 1)
+        sol_err = float(np.linalg.norm(x.numpy() - xo[dids]) / np.linalg.norm(xo[dids]))
+        q.put((rank, sol_err, it, ito10, res, status, pcg.replacements))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,nel", [(2, (8, 3, 3)), (3, (9, 3, 2))])
+def test_slab_mixed_pcg_matches_single_domain(world, nel):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main_mixed, args=(r, world, port, nel, q)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for rank, sol_err, it, ito, res, status, repl in out:
+        assert status == "ok" and res < 1e-10, (rank, status, res)
+        assert sol_err < 1e-8, (rank, sol_err)
+        assert repl >= 1
+        # FP32 inner iterations with replacement stay near the FP64 count
+        assert it <= 1.5 * ito + 10, (it, ito)
+    # every rank stopped at the same iteration (the stopping test is global)
+    assert len({o[2] for o in out}) == 1
 
 
 def test_partition():
